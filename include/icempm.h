@@ -1,0 +1,247 @@
+/*
+ * icempm.h -- C ABI of the B200-native 2D APIC MPM sea-ice step.
+ *
+ * This is the drop-in boundary for the reference's GPU driver path
+ * (simulation/gpu_implementation5.{h,cpp}, simulation/gpu_partition.{h,cpp},
+ * simulation/kernels.cuh of igorg520b/iceMPM_2d_sp).  Every entry point takes
+ * plain pointers and sizes; no C++ or torch types cross it.  The caller owns
+ * all host buffers; the library owns the device arrays and its CUDA stream.
+ *
+ * Return convention (all functions): 0 = ok, negative = API/CUDA error
+ * (ICEMPM_E_*; icempm_last_error() gives the message of the calling thread).
+ * Device-side simulation errors are reported separately as the reference's
+ * bitmask (ICEMPM_ERR_*) through icempm_get_status().
+ *
+ * Threading: a handle is not re-entrant; calls on one handle must be
+ * serialised by the caller (the reference drives GPU_Implementation5 from a
+ * single thread: cli/main.cpp:55-59, gui/backgroundworker.cpp:37-63).
+ * Separate handles are independent.
+ */
+#ifndef ICEMPM_H
+#define ICEMPM_H
+
+#include <stddef.h>
+#include <stdint.h>
+#ifndef __cplusplus
+#include <stdbool.h>
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* SimParams: byte-for-byte mirror of `struct SimParams`                    */
+/* (simulation/parameters_sim.h:36-127).  Field order, types and therefore  */
+/* the x86-64 layout (328 bytes) are identical, so a caller holding the     */
+/* reference struct can pass its address directly.  The static members of  */
+/* the reference struct are the ICEMPM_* constants below.                   */
+/* ------------------------------------------------------------------------ */
+typedef struct icempm_simparams {
+    int32_t tpb_P2G, tpb_Upd, tpb_G2P;
+    uint32_t nPartitions;
+    int32_t nPtsInitial;
+    int64_t SimulationStartUnixTime;
+    double InitialTimeStep, SimulationEndTime;
+    double AnimationFramePeriod;
+    int32_t SimulationStep;
+    double SimulationTime;
+    bool SaveSnapshots;
+    int32_t SnapshotPeriod;
+    int32_t GridXTotal, GridYTotal;
+    int32_t ModeledRegionOffsetX, ModeledRegionOffsetY;
+    int32_t InitializationImageSizeX, InitializationImageSizeY;
+    double DimensionHorizontal;
+    double windDragCoeff_airDensity;
+    bool UseWindData, UseCurrentData;
+    double sea_water_density;
+    double waterDragEffectiveLinear, waterDragEffectiveQuadratic;
+    double IceDensity, PoissonsRatio, YoungsModulus;
+    double IceCompressiveStrength, IceTensileStrength, IceShearStrength, IceTensileStrength2;
+    double DP_phi, DP_threshold_p;
+    double RidgeFormationCoeff;
+    double cellsize;
+    double ParticleVolume, ParticleViewSize;
+    double dt_vol_Dpinv, vmax;
+    double lambda, mu, kappa;
+    double ParticleMass;
+    double cellsize_inv, Dp_inv;
+    int32_t UpdateEveryNthStep;
+} icempm_simparams_t;
+
+/* static constexpr members of SimParams (parameters_sim.h:39-76) */
+#define ICEMPM_DISABLED_PTS_PROPORTION_THRESHOLD 0.05f
+#define ICEMPM_PI 3.14159265358979323846
+#define ICEMPM_GRAVITY 9.8
+#define ICEMPM_MAX_REGIONS 100
+
+/* grid arrays (parameters_sim.h:49-58); node index = y + x*GridYTotal */
+enum {
+    ICEMPM_GRID_MASS = 0, ICEMPM_GRID_PX = 1, ICEMPM_GRID_PY = 2,
+    ICEMPM_GRID_NX = 3, ICEMPM_GRID_NY = 4,
+    ICEMPM_GRID_CURRENT_VX = 5, ICEMPM_GRID_CURRENT_VY = 6,
+    ICEMPM_GRID_FX = 7, ICEMPM_GRID_FY = 8,
+    ICEMPM_N_GRID_ARRAYS = 9
+};
+
+/* HSSOA rows (parameters_sim.h:65-76): point i, row j lives at
+ * buf[i + capacity*j], all rows f64.  Rows 0-2 hold a uint32 in the low 4
+ * bytes of the double slot (the reference reinterpret_casts them). */
+enum {
+    ICEMPM_IDX_UTILITY = 0, ICEMPM_IDX_CELL = 1, ICEMPM_IDX_POINT = 2,
+    ICEMPM_IDX_P = 3, ICEMPM_IDX_Q = 4, ICEMPM_IDX_JP_INV = 5,
+    ICEMPM_IDX_POSX = 6, ICEMPM_IDX_VELX = 8, ICEMPM_IDX_FE00 = 10,
+    ICEMPM_IDX_BP00 = 14, ICEMPM_IDX_THICKNESS = 18,
+    ICEMPM_N_PTS_ARRAYS = 19
+};
+
+/* point flags in the utility word (kernels.cuh:11-13) */
+#define ICEMPM_STATUS_CRUSHED  0x10000u
+#define ICEMPM_STATUS_DISABLED 0x20000u
+#define ICEMPM_STATUS_ERROR    0x40000u
+
+/* device error bitmask, same values as kernels.cuh:17-26 */
+#define ICEMPM_ERR_POINT_POS_NAN      0x0001u
+#define ICEMPM_ERR_POINT_VEL_NAN      0x0002u
+#define ICEMPM_ERR_POINT_JUMP_CELLS   0x0004u
+#define ICEMPM_ERR_POINT_LEFT_AREA    0x0008u
+#define ICEMPM_ERR_POINT_BP_NAN       0x0010u
+#define ICEMPM_ERR_POINT_FE_NAN       0x0020u
+#define ICEMPM_ERR_GRID_P2G_NAN_VEL   0x0100u
+#define ICEMPM_ERR_GRID_P2G_NAN_MASS  0x0200u
+#define ICEMPM_ERR_GRID_NAN           0x0400u
+/* bits added by this library (no reference counterpart) */
+#define ICEMPM_ERR_FIXED_OVERFLOW     0x1000u  /* a P2G term exceeded the fixed-point range */
+#define ICEMPM_ERR_BARRIER_TIMEOUT    0x2000u  /* a bounded device wait gave up */
+
+/* API error codes (negative returns) */
+#define ICEMPM_OK            0
+#define ICEMPM_E_ARG        (-1)
+#define ICEMPM_E_CUDA       (-2)
+#define ICEMPM_E_NOMEM      (-3)
+#define ICEMPM_E_STATE      (-4)
+#define ICEMPM_E_CAPACITY   (-5)
+#define ICEMPM_E_UNSUPPORTED (-6)
+
+/* ------------------------------------------------------------------------ */
+/* Options (no reference counterpart: the reference has one FP64 path).      */
+/* ------------------------------------------------------------------------ */
+enum {
+    ICEMPM_VARIANT_FIXED = 0, /* FP32 state, int64 fixed-point P2G (deterministic) */
+    ICEMPM_VARIANT_FP32  = 1, /* FP32 state, FP32 atomics                           */
+    ICEMPM_VARIANT_FP64  = 2  /* FP64 state and arithmetic, FP64 atomics            */
+};
+enum {
+    ICEMPM_FORCING_COMPAT   = 0, /* reference grid update: effective drag + current ramp (kernels.cuh:141-169) */
+    ICEMPM_FORCING_EXTENDED = 1  /* quadratic water drag (rho_w, Cd) + wind stress (rho_a, Ca) */
+};
+enum { ICEMPM_WIND_NONE = 0, ICEMPM_WIND_UNIFORM = 1, ICEMPM_WIND_RANKINE = 2 };
+
+typedef struct icempm_options {
+    int32_t variant;          /* ICEMPM_VARIANT_* */
+    int32_t forcing;          /* ICEMPM_FORCING_* */
+    int32_t sort_every;       /* internal locality re-sort cadence in steps; 0 = only at upload */
+    int32_t use_graphs;       /* capture step chunks in CUDA graphs (1 = yes) */
+    int32_t block_threads;    /* particle kernel CTA size: 128, 256 or 512 (0 = default) */
+    int32_t warp_reduce;      /* same-cell warp pre-reduction in P2G (1 = yes) */
+    int32_t device;           /* CUDA device ordinal */
+    int32_t reserved0;
+    /* extended forcing only */
+    double water_density, water_drag_coeff;   /* rho_w [kg/m^3], Cd */
+    double air_density, air_drag_coeff;       /* rho_a [kg/m^3], Ca */
+    int32_t wind_kind;                        /* ICEMPM_WIND_* */
+    int32_t reserved1;
+    double wind_u, wind_v;                    /* uniform wind [m/s] */
+    double wind_cx, wind_cy;                  /* Rankine centre [m, world coords] */
+    double wind_vmax, wind_radius;            /* Rankine peak speed [m/s] and radius [m] */
+} icempm_options_t;
+
+typedef struct icempm_context icempm_t;
+
+/* Fill `opts` with the defaults (fixed-point variant, compat forcing). */
+void icempm_default_options(icempm_options_t *opts);
+
+/* Create a context for one scene on one GPU.
+ * Replaces GPU_Implementation5::initialize + GPU_Partition::allocate +
+ * transfer_grid_data_to_device + update_current_field
+ * (gpu_implementation5.cpp:94-128,165-184; gpu_partition.cpp:108-137,174-196,259-293).
+ *   prms          : SimParams with helper variables computed (ComputeHelperVariables)
+ *   grid_status   : GridX*GridY bytes, node index y + x*GridY (100 = modelled water)
+ *   current_vxvy  : 2*GridX*GridY doubles (vx block then vy block) or NULL (zero current)
+ *   capacity      : maximum number of points the device arrays hold
+ *   opts          : NULL for defaults */
+int icempm_create(const icempm_simparams_t *prms, const uint8_t *grid_status,
+                  const double *current_vxvy, uint32_t capacity,
+                  const icempm_options_t *opts, icempm_t **out);
+
+/* Destroy a context and free its device memory (GPU_Partition::~GPU_Partition,
+ * gpu_partition.cpp:214-232). NULL is accepted. */
+int icempm_destroy(icempm_t *ctx);
+
+/* Upload `size` points from a reference-layout HSSOA buffer (19 rows of
+ * `capacity` doubles).  Replaces GPU_Partition::transfer_points_from_soa_to_device
+ * (gpu_partition.cpp:81-106).  disabled_count seeds the device counter. */
+int icempm_upload_points(icempm_t *ctx, const double *hssoa, uint32_t capacity,
+                         uint32_t size, int32_t disabled_count);
+
+/* Re-read SimParams (GPU_Partition::update_constants, gpu_partition.cpp:140-170).
+ * Also clears the device error word as the reference does. */
+int icempm_update_constants(icempm_t *ctx, const icempm_simparams_t *prms);
+
+/* Replace the current field (GPU_Partition::update_current_field,
+ * gpu_partition.cpp:174-196): 2*GridX*GridY doubles, vx block then vy block. */
+int icempm_set_current(icempm_t *ctx, const double *current_vxvy);
+
+/* Advance `nsteps` sub-steps starting at step index `first_step`.  Step k runs
+ * reset_grid, p2g, update_nodes(t = dt*k rounded to float) and
+ * g2p(recordPQ = (k % UpdateEveryNthStep == 0)), exactly as the loop in
+ * Model::Step (model.cpp:18-39).  Asynchronous: returns after enqueueing. */
+int icempm_step(icempm_t *ctx, int32_t nsteps, int32_t first_step);
+
+/* Download all points into a reference-layout HSSOA buffer, in the slot order
+ * of the last upload (or of the last icempm_sort_compact).  Replaces
+ * GPU_Partition::transfer_from_device's point part (gpu_partition.cpp:17-38).
+ * Synchronises the stream.  *size receives the number of points. */
+int icempm_download_points(icempm_t *ctx, double *hssoa, uint32_t capacity, uint32_t *size);
+
+/* Fetch the device error bitmask and disabled-point counter
+ * (gpu_partition.cpp:40-48).  Synchronises the stream. */
+int icempm_get_status(icempm_t *ctx, uint32_t *error_bits, int32_t *disabled_count);
+
+/* Zero the boundary-force accumulators (GPU_Partition::clear_force_accumulator,
+ * gpu_partition.cpp:310-319). */
+int icempm_clear_force_accumulator(icempm_t *ctx);
+
+/* Download the accumulated boundary forces into fxfy (2*GridX*GridY doubles,
+ * fx block then fy block) divided by elapsed_steps*dt, as
+ * GPU_Implementation5::transfer_from_device does (gpu_implementation5.cpp:188-224). */
+int icempm_get_boundary_forces(icempm_t *ctx, double *fxfy, int32_t elapsed_steps);
+
+/* Remove disabled points and sort the rest by cell index x*GridY+y, on the
+ * device.  Same result as HostSideSOA::RemoveDisabledAndSort followed by a
+ * re-upload (host_side_soa.cpp:36-47, model.cpp:63-72); ties keep their
+ * previous relative order.  Resets the disabled counter to 0. */
+int icempm_sort_compact(icempm_t *ctx);
+
+/* Device time of the last icempm_step call, in ms: [0] total, [1] grid
+ * update kernels, [2] fused G2P+P2G kernels, [3] locality re-sorts.
+ * Synchronises the stream. (GPU_Partition::record_timings, gpu_partition.cpp:370-436) */
+int icempm_timings(icempm_t *ctx, float ms[4]);
+
+/* Number of points currently on the device (including disabled ones). */
+int icempm_point_count(icempm_t *ctx, uint32_t *n);
+
+/* CUDA stream the context enqueues on (cudaStream_t), for event timing. */
+int icempm_get_stream(icempm_t *ctx, void **stream);
+
+/* Number of kernel launches this context has enqueued since creation. */
+int icempm_launch_count(icempm_t *ctx, uint64_t *count);
+
+/* Message of the last failing call on this thread ("" if none). */
+const char *icempm_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ICEMPM_H */

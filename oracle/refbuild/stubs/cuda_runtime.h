@@ -1,0 +1,24 @@
+/* Host stand-in for <cuda_runtime.h>, used only to compile the reference's
+ * kernels.cuh / helper_math.cuh / givens.cuh as plain host C++ for the oracle
+ * pin.  Kernels become ordinary functions that the harness calls once per
+ * (block, thread) in index order; atomics become plain read-modify-writes. */
+#pragma once
+#include <math.h>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <algorithm>
+#define __host__
+#define __device__
+#define __global__
+#define __constant__
+#define __forceinline__ inline
+struct ref_dim3 { unsigned x = 0, y = 0, z = 0; };
+extern ref_dim3 blockIdx, threadIdx, blockDim;
+inline double atomicAdd(double *a, double v) { double o = *a; *a = o + v; return o; }
+inline float atomicAdd(float *a, float v) { float o = *a; *a = o + v; return o; }
+inline int atomicAdd(int *a, int v) { int o = *a; *a = o + v; return o; }
+using std::min;
+using std::max;
+typedef int cudaError_t;

@@ -1,0 +1,348 @@
+#!/usr/bin/env python
+"""Throughput benchmark of the B200-native 2D APIC MPM step (particle-steps/s).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (default): the "plain MPM at scale" scene -- 4096x2048 grid, h=1 m,
+2000 uniform Voronoi seeds with 70% of the floes kept, 4 points per cell with
++-0.25h jitter, lognormal(0, 0.3) thickness per floe, Rankine-vortex wind
+(20 m/s at 800 cells), uniform 0.1 m/s current, dt=1e-4 s (seeded, synthetic).
+One "step" is one MPM sub-step (grid update + fused G2P/P2G) of the whole scene.
+
+Our arm: the chosen form (fixed-point P2G, FP32 state) is timed for K steps
+with CUDA events on the library's stream (one event pair around every kernel
+and one around the whole region), the plain FP32-atomic form beside it, an
+end-to-end run through the C ABI with pinned host buffers, and the FP64 CPU
+oracle on the host cores.  Under torchrun every rank runs its own scene
+(different seed: weak scaling, no collective in the step); rank 0 prints one
+JSON line with the whole-job throughput (max time over ranks).
+
+--impl reference: the reference's own kernels (simulation/kernels.cuh,
+compiled for the host in oracle/_ref) advance a bounded sample of the same
+scene family on the host cores; rank 0 only.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-steps/s on 1 B200, chosen vs plain at ≤1e-4 err vs FP64; % HBM peak"
+UNIT = "particle-steps/s"
+WORKLOAD = ("config1: plain MPM at scale, 4096x2048 grid, h=1 m, 2000 Voronoi floes (70% kept), "
+            "4 ppc +-0.25h jitter, lognormal(0,0.3) thickness, Rankine wind 20 m/s @ 800 cells, dt=1e-4 s")
+FALLBACK_HBM_GBS = 6650.0
+# algorithmic bytes per step: 124 per point + 49 per grid node (FP32/u32 words,
+# each word the step consumes read once and each word it modifies written once)
+B_POINT, B_NODE = 124, 49
+# split of the node bytes: the fused G2P+P2G kernel reads 8 B of velocity and
+# flushes 12 B of accumulators per node; the grid update moves the other 29 B
+B_NODE_FUSED = 20
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--max-points", type=int, default=None,
+                    help="keep whole floes until this many points (the ~8.4M-point variant)")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--cpu-steps", type=int, default=4)
+    return ap.parse_args()
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.index), "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.t = threading.Thread(target=self._read, daemon=True)
+        self.t.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append((time.time(), [c.strip() for c in line.split(",")]))
+
+    def mark(self):
+        return time.time()
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self, t0, t1):
+        rows = [r for t, r in self.rows if t0 - 0.15 <= t <= t1 + 0.15] or [r for _, r in self.rows[-3:]]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if len(r) > 5 + k and r[5 + k] == "Active"})
+        pw = [float(r[3]) for r in rows if r[3].replace(".", "").isdigit()]
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows), "power_w_max": max(pw) if pw else None}
+
+
+def make_scene(seed, max_points=None, sample=False):
+    from icempm_2d_sp_b200 import scenes
+    if sample:  # the same generation rules on a 1024x512 sub-domain (1/16 of the cells)
+        return scenes.config1(seed=seed, gx=1024, gy=512, n_seeds=125)
+    return scenes.config1(seed=seed, max_points=max_points)
+
+
+def run_reference(args, rank):
+    """The reference kernels on the host cores, one sub-step of the sample
+    scene per step."""
+    if rank != 0:
+        return
+    sc = make_scene(1235, sample=True)
+    grid = np.zeros((9, sc.grid_nodes))
+    grid[5], grid[6] = sc.current[:sc.grid_nodes], sc.current[sc.grid_nodes:]
+    sample = (f"config1 generation rules on a 1024x512 sub-domain (125 seeds), N={sc.n} points, "
+              f"one sub-step per step")
+    try:
+        from oracle.refbuild import build_ref
+        L = build_ref.load()
+        cores = int(L.ref_num_threads())
+        kind = "reference"
+        run = lambda k, first: build_ref.run_steps(sc.prms, sc.soa, sc.n, grid, sc.status, k, first)
+        note = ("reference simulation/kernels.cuh compiled for the host (oracle/_ref); P2G serial "
+                "(its atomics emulated in order), grid update and G2P over OpenMP threads; "
+                "compat forcing (the reference has no wind term)")
+    except (FileNotFoundError, OSError):
+        import oracle
+        cores = oracle.num_threads()
+        kind = "port"
+        run = lambda k, first: oracle.run_steps(sc.prms, sc.soa, sc.n, grid, sc.status, k, first)
+        note = "FP64 oracle port (OpenMP); the reference build was not available"
+    run(args.warmup, 0)
+    t0 = time.perf_counter()
+    run(args.steps, args.warmup)
+    dt = time.perf_counter() - t0
+    v = sc.n * args.steps / dt
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": WORKLOAD, "points": int(sc.n), "grid_nodes": sc.grid_nodes},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample, "note": note},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline(args, sc):
+    import oracle
+    soa = sc.soa.copy()
+    grid = np.zeros((9, sc.grid_nodes))
+    grid[5], grid[6] = sc.current[:sc.grid_nodes], sc.current[sc.grid_nodes:]
+    k = max(1, args.cpu_steps)
+    t0 = time.perf_counter()
+    oracle.run_steps(sc.prms, soa, sc.n, grid, sc.status, k, 0, opts=sc.options)
+    dt = time.perf_counter() - t0
+    return {"value": sc.n * k / dt, "unit": UNIT, "cores": oracle.num_threads(), "kind": "port",
+            "sample": f"the full benchmark scene (N={sc.n}) for {k} sub-steps with the FP64 OpenMP oracle"}
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+
+    import torch
+    from icempm_2d_sp_b200 import capi
+    from icempm_2d_sp_b200.params import Options, VARIANT_FIXED, VARIANT_FP32
+
+    def sync_all():
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+
+    sc = make_scene(1235 + rank, max_points=args.max_points)
+    n, G = sc.n, sc.grid_nodes
+    peak, peak_src = load_peaks()
+
+    def timed(variant):
+        o = Options.default(forcing=sc.options.forcing)
+        for f, _ in Options._fields_:
+            setattr(o, f, getattr(sc.options, f))
+        o.variant, o.device, o.use_graphs = variant, local, 1
+        with capi.Context(sc.prms, sc.status, sc.current, capacity=n, options=o) as ctx:
+            ctx.upload(sc.soa, n)
+            ctx.step(args.warmup, 0)
+            sync_all()
+            l0 = ctx.launch_count()
+            sampler = ClockSampler(local)
+            sampler.start()
+            time.sleep(0.3)
+            t0 = time.time()
+            upd, fused = ctx.phase_times(args.steps)
+            t1 = time.time()
+            total = ctx.timings()[0]
+            time.sleep(0.2)
+            sampler.stop()
+            sync_all()
+            launches = ctx.launch_count() - l0
+            err, dis = ctx.status()
+        return total, upd, fused, launches, sampler.summary(t0, t1), err
+
+    total, upd, fused, launches, clocks, err = timed(VARIANT_FIXED)
+    t_ms = total
+    n_tot = n
+    if dist:
+        t = torch.tensor([t_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_ms = float(t.item())
+        c = torch.tensor([float(n)], device="cuda", dtype=torch.float64)
+        dist.all_reduce(c, op=dist.ReduceOp.SUM)
+        n_tot = int(c.item())
+    value = n_tot * args.steps / (t_ms * 1e-3)
+
+    plain = None
+    if not args.no_plain:
+        ptot, pupd, pfused, _, _, _ = timed(VARIANT_FP32)
+        plain = {"value": n * args.steps / (ptot * 1e-3), "ms_per_step": ptot / args.steps,
+                 "fused_kernel_ms": pfused / args.steps, "variant": "fp32 atomics (plain)"}
+
+    # roofline of the dominant kernel (fused G2P+P2G), live events of the timed region
+    fused_bytes = B_POINT * n + B_NODE_FUSED * G
+    fused_launch_s = fused * 1e-3 / args.steps
+    achieved = fused_bytes / fused_launch_s / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "fused_kernel_traffic.json")
+    if os.path.exists(tp):
+        with open(tp) as f:
+            td = json.load(f)
+        traffic = td["bytes_per_point"] * n + td["bytes_per_node"] * G
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic, "peak_source": peak_src,
+                "kernel": "k_g2p_p2g (fused G2P + P2G)", "algorithmic_bytes_per_launch": fused_bytes,
+                "avg_launch_ms": fused * 1e-3 / args.steps * 1e3,
+                "step_bytes": B_POINT * n + B_NODE * G,
+                "step_achieved_gbs": (B_POINT * n + B_NODE * G) / (total * 1e-3 / args.steps) / 1e9,
+                "grid_update_avg_ms": upd / args.steps}
+
+    e2e = None
+    if not args.no_e2e:
+        e2e = end_to_end(args, sc, local, capi, Options, VARIANT_FIXED)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(args, sc)
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded scene generator, BASELINE config 1 rules)",
+                "config": {"workload": WORKLOAD, "points": int(n), "points_all_ranks": n_tot, "grid_nodes": G,
+                           "variant": "fixed: int64 fixed-point P2G, FP32 state (chosen form)",
+                           "forcing": "extended (Rankine wind, quadratic water drag)",
+                           "parallelism": f"{world} independent scene(s), one per GPU",
+                           "l2": "inputs larger than L2 (2.0 GB point state, 0.4 GB grid)",
+                           "device_errors": err},
+                "plain": plain, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+                "gpu_launches": launches, "clocks": clocks}
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def end_to_end(args, sc, local, capi, Options, variant):
+    """The reference-facing call sequence through the C ABI with host buffers:
+    upload the HSSOA from page-locked memory, then frames of UpdateEveryNthStep
+    sub-steps, each followed by the download of the HSSOA, the status word and
+    the boundary forces (Model::Step, model.cpp:7-78)."""
+    import torch
+    n, G = sc.n, sc.grid_nodes
+    src = sc.soa
+    dst = np.zeros_like(src)
+    capi.host_register(src)
+    capi.host_register(dst)
+    o = Options.default()
+    for f, _ in Options._fields_:
+        setattr(o, f, getattr(sc.options, f))
+    o.variant, o.device = variant, local
+    frame = sc.prms.UpdateEveryNthStep
+    try:
+        with capi.Context(sc.prms, sc.status, sc.current, capacity=n, options=o) as ctx:
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            ctx.upload(src, n)
+            done, frames = 0, 0
+            while done < args.steps:
+                k = min(frame, args.steps - done)
+                ctx.clear_force_accumulator()
+                ctx.step(k, done)
+                ctx.download(dst)
+                ctx.status()
+                ctx.boundary_forces(k)
+                done += k
+                frames += 1
+            t1 = time.perf_counter()
+    finally:
+        capi.host_unregister(src)
+        capi.host_unregister(dst)
+    hssoa_bytes = 19 * 8 * n
+    return {"value": n * args.steps / (t1 - t0), "unit": UNIT,
+            "h2d_bytes_per_step": hssoa_bytes / args.steps,
+            "d2h_bytes_per_step": frames * (hssoa_bytes + 16 * G + 8) / args.steps,
+            "frames": frames, "frame_steps": frame,
+            "note": "upload from page-locked host memory, per frame: step + HSSOA download + status + boundary forces"}
+
+
+if __name__ == "__main__":
+    main()

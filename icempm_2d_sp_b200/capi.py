@@ -1,0 +1,208 @@
+"""ctypes binding of the C ABI (include/icempm.h) in libicempm_b200.so.
+
+The library is built in-tree (icempm_2d_sp_b200/build.py).  Loading fails
+loudly when it is missing: there is no CPU fallback.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from .params import SimParams, Options, N_PTS_ARRAYS
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libicempm_b200.so")
+
+EXPORTS = [
+    "icempm_default_options", "icempm_create", "icempm_destroy", "icempm_upload_points",
+    "icempm_update_constants", "icempm_set_current", "icempm_step", "icempm_download_points",
+    "icempm_get_status", "icempm_clear_force_accumulator", "icempm_get_boundary_forces",
+    "icempm_sort_compact", "icempm_timings", "icempm_phase_times", "icempm_fixed_point_scales",
+    "icempm_host_register", "icempm_host_unregister", "icempm_device_count", "icempm_point_count",
+    "icempm_get_stream", "icempm_launch_count", "icempm_last_error",
+]
+
+
+class IcempmError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"icempm error {code}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def load(path: str = LIB_PATH):
+    """Load the CUDA library (no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(f"{path} is missing: build it with `python -m icempm_2d_sp_b200.build`")
+    L = C.CDLL(path)
+    h = C.c_void_p
+    sp, op = C.POINTER(SimParams), C.POINTER(Options)
+    dp, u8p = C.POINTER(C.c_double), C.POINTER(C.c_uint8)
+    sig = {
+        "icempm_default_options": (None, [op]),
+        "icempm_create": (C.c_int, [sp, u8p, dp, C.c_uint32, op, C.POINTER(h)]),
+        "icempm_destroy": (C.c_int, [h]),
+        "icempm_upload_points": (C.c_int, [h, dp, C.c_uint32, C.c_uint32, C.c_int32]),
+        "icempm_update_constants": (C.c_int, [h, sp]),
+        "icempm_set_current": (C.c_int, [h, dp]),
+        "icempm_step": (C.c_int, [h, C.c_int32, C.c_int32]),
+        "icempm_download_points": (C.c_int, [h, dp, C.c_uint32, C.POINTER(C.c_uint32)]),
+        "icempm_get_status": (C.c_int, [h, C.POINTER(C.c_uint32), C.POINTER(C.c_int32)]),
+        "icempm_clear_force_accumulator": (C.c_int, [h]),
+        "icempm_get_boundary_forces": (C.c_int, [h, dp, C.c_int32]),
+        "icempm_sort_compact": (C.c_int, [h]),
+        "icempm_timings": (C.c_int, [h, C.POINTER(C.c_float)]),
+        "icempm_phase_times": (C.c_int, [h, C.c_int32, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+        "icempm_fixed_point_scales": (C.c_int, [h, dp, dp]),
+        "icempm_host_register": (C.c_int, [C.c_void_p, C.c_size_t]),
+        "icempm_host_unregister": (C.c_int, [C.c_void_p]),
+        "icempm_device_count": (C.c_int, [C.POINTER(C.c_int)]),
+        "icempm_point_count": (C.c_int, [h, C.POINTER(C.c_uint32)]),
+        "icempm_get_stream": (C.c_int, [h, C.POINTER(C.c_void_p)]),
+        "icempm_launch_count": (C.c_int, [h, C.POINTER(C.c_uint64)]),
+        "icempm_last_error": (C.c_char_p, []),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = L
+    return L
+
+
+def check(rc):
+    if rc < 0:
+        raise IcempmError(rc, _lib.icempm_last_error().decode())
+    return rc
+
+
+def _dp(a):
+    if a is None:
+        return None
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def device_count() -> int:
+    L = load()
+    n = C.c_int(0)
+    L.icempm_device_count(C.byref(n))
+    return n.value
+
+
+def host_register(arr: np.ndarray) -> None:
+    check(load().icempm_host_register(arr.ctypes.data, arr.nbytes))
+
+
+def host_unregister(arr: np.ndarray) -> None:
+    check(load().icempm_host_unregister(arr.ctypes.data))
+
+
+class Context:
+    """One scene on one GPU behind the C ABI (the role of GPU_Implementation5)."""
+
+    def __init__(self, prms: SimParams, grid_status: np.ndarray, current=None, capacity: int = 0,
+                 options: Options = None):
+        L = load()
+        self._L = L
+        self.prms = prms.copy()
+        self.options = options if options is not None else Options.default()
+        st = np.ascontiguousarray(grid_status, dtype=np.uint8)
+        assert st.size == prms.GridXTotal * prms.GridYTotal
+        cur = None if current is None else np.ascontiguousarray(current, dtype=np.float64)
+        self.G = prms.GridXTotal * prms.GridYTotal
+        h = C.c_void_p()
+        check(L.icempm_create(C.byref(self.prms), st.ctypes.data_as(C.POINTER(C.c_uint8)), _dp(cur),
+                              int(capacity), C.byref(self.options), C.byref(h)))
+        self.h = h
+        self.capacity = int(capacity)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self._L.icempm_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def upload(self, soa: np.ndarray, n: int, disabled: int = 0):
+        assert soa.shape[0] == N_PTS_ARRAYS
+        check(self._L.icempm_upload_points(self.h, _dp(soa), soa.shape[1], int(n), int(disabled)))
+
+    def update_constants(self, prms: SimParams):
+        self.prms = prms.copy()
+        check(self._L.icempm_update_constants(self.h, C.byref(self.prms)))
+
+    def set_current(self, current):
+        cur = None if current is None else np.ascontiguousarray(current, dtype=np.float64)
+        check(self._L.icempm_set_current(self.h, _dp(cur)))
+
+    def step(self, nsteps: int, first_step: int = 0):
+        check(self._L.icempm_step(self.h, int(nsteps), int(first_step)))
+
+    def download(self, soa: np.ndarray = None) -> tuple:
+        if soa is None:
+            soa = np.zeros((N_PTS_ARRAYS, max(self.count(), 1)), np.float64)
+        n = C.c_uint32(0)
+        check(self._L.icempm_download_points(self.h, _dp(soa), soa.shape[1], C.byref(n)))
+        return soa, n.value
+
+    def status(self) -> tuple:
+        e, d = C.c_uint32(0), C.c_int32(0)
+        check(self._L.icempm_get_status(self.h, C.byref(e), C.byref(d)))
+        return e.value, d.value
+
+    def clear_force_accumulator(self):
+        check(self._L.icempm_clear_force_accumulator(self.h))
+
+    def boundary_forces(self, elapsed_steps: int) -> np.ndarray:
+        out = np.zeros(2 * self.G)
+        check(self._L.icempm_get_boundary_forces(self.h, _dp(out), int(elapsed_steps)))
+        return out
+
+    def sort_compact(self):
+        check(self._L.icempm_sort_compact(self.h))
+
+    def timings(self):
+        ms = (C.c_float * 4)()
+        check(self._L.icempm_timings(self.h, ms))
+        return list(ms)
+
+    def phase_times(self, nsteps: int):
+        u, f = C.c_float(0), C.c_float(0)
+        check(self._L.icempm_phase_times(self.h, int(nsteps), C.byref(u), C.byref(f)))
+        return u.value, f.value
+
+    def fixed_point_scales(self):
+        a, b = C.c_double(0), C.c_double(0)
+        check(self._L.icempm_fixed_point_scales(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def count(self) -> int:
+        n = C.c_uint32(0)
+        check(self._L.icempm_point_count(self.h, C.byref(n)))
+        return n.value
+
+    def stream(self) -> int:
+        s = C.c_void_p()
+        check(self._L.icempm_get_stream(self.h, C.byref(s)))
+        return s.value or 0
+
+    def launch_count(self) -> int:
+        c = C.c_uint64(0)
+        check(self._L.icempm_launch_count(self.h, C.byref(c)))
+        return c.value

@@ -1,0 +1,239 @@
+// capi.cu -- the extern "C" boundary declared in include/icempm.h.
+// Each entry point validates its arguments, forwards to the variant engine and
+// turns failures into negative return codes with a per-thread message; no C++
+// exception crosses the boundary.
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "engine_iface.h"
+
+namespace icempm {
+static thread_local std::string g_last_error;
+int fail(int code, const std::string &msg)
+{
+    g_last_error = msg;
+    return code;
+}
+}  // namespace icempm
+
+using icempm::fail;
+
+struct icempm_context {
+    icempm::Engine *eng = nullptr;
+    icempm_simparams_t prms{};
+    icempm_options_t opts{};
+};
+
+#define ICEMPM_GUARD_CTX(ctx) \
+    if (!(ctx) || !(ctx)->eng) return fail(ICEMPM_E_ARG, "null context")
+
+#define ICEMPM_TRY(expr)                                                   \
+    try {                                                                  \
+        return (expr);                                                     \
+    } catch (const std::bad_alloc &) {                                     \
+        return fail(ICEMPM_E_NOMEM, "host allocation failed");             \
+    } catch (const std::exception &e) {                                    \
+        return fail(ICEMPM_E_STATE, e.what());                             \
+    } catch (...) {                                                        \
+        return fail(ICEMPM_E_STATE, "unknown exception");                  \
+    }
+
+extern "C" {
+
+void icempm_default_options(icempm_options_t *o)
+{
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->variant = ICEMPM_VARIANT_FIXED;
+    o->forcing = ICEMPM_FORCING_COMPAT;
+    o->sort_every = 0;
+    o->use_graphs = 1;
+    o->block_threads = 256;
+    o->warp_reduce = 1;
+    o->device = 0;
+    o->water_density = 1025.0;
+    o->water_drag_coeff = 5.5e-3;
+    o->air_density = 1.3;
+    o->air_drag_coeff = 1.2e-3;
+    o->wind_kind = ICEMPM_WIND_NONE;
+}
+
+int icempm_create(const icempm_simparams_t *prms, const uint8_t *grid_status, const double *current_vxvy,
+                  uint32_t capacity, const icempm_options_t *opts, icempm_t **out)
+{
+    if (!out) return fail(ICEMPM_E_ARG, "out is null");
+    *out = nullptr;
+    if (!prms || !grid_status) return fail(ICEMPM_E_ARG, "prms and grid_status are required");
+    icempm_options_t o;
+    if (opts) o = *opts; else icempm_default_options(&o);
+    if (o.block_threads != 0 && o.block_threads != 256)
+        return fail(ICEMPM_E_UNSUPPORTED, "block_threads must be 0 or 256");
+    if (o.forcing != ICEMPM_FORCING_COMPAT && o.forcing != ICEMPM_FORCING_EXTENDED)
+        return fail(ICEMPM_E_ARG, "unknown forcing");
+    icempm::Engine *e = nullptr;
+    switch (o.variant) {
+    case ICEMPM_VARIANT_FIXED: e = icempm::make_engine_fixed(); break;
+    case ICEMPM_VARIANT_FP32: e = icempm::make_engine_fp32(); break;
+    case ICEMPM_VARIANT_FP64: e = icempm::make_engine_fp64(); break;
+    default: return fail(ICEMPM_E_ARG, "unknown variant");
+    }
+    icempm_context *c = new (std::nothrow) icempm_context;
+    if (!c) { delete e; return fail(ICEMPM_E_NOMEM, "context allocation failed"); }
+    c->eng = e;
+    c->prms = *prms;
+    c->opts = o;
+    int rc;
+    try {
+        rc = e->init(*prms, grid_status, current_vxvy, capacity, o);
+    } catch (...) {
+        rc = fail(ICEMPM_E_STATE, "exception during init");
+    }
+    if (rc) { delete e; delete c; return rc; }
+    *out = c;
+    icempm::g_last_error.clear();
+    return ICEMPM_OK;
+}
+
+int icempm_destroy(icempm_t *ctx)
+{
+    if (!ctx) return ICEMPM_OK;
+    delete ctx->eng;
+    delete ctx;
+    return ICEMPM_OK;
+}
+
+int icempm_upload_points(icempm_t *ctx, const double *hssoa, uint32_t capacity, uint32_t size, int32_t disabled_count)
+{
+    ICEMPM_GUARD_CTX(ctx);
+    if (!hssoa && size) return fail(ICEMPM_E_ARG, "hssoa is null");
+    ICEMPM_TRY(ctx->eng->upload(hssoa, capacity, size, disabled_count));
+}
+
+int icempm_update_constants(icempm_t *ctx, const icempm_simparams_t *prms)
+{
+    ICEMPM_GUARD_CTX(ctx);
+    if (!prms) return fail(ICEMPM_E_ARG, "prms is null");
+    if (prms->GridXTotal != ctx->prms.GridXTotal || prms->GridYTotal != ctx->prms.GridYTotal)
+        return fail(ICEMPM_E_ARG, "grid size cannot change after create");
+    ctx->prms = *prms;
+    ICEMPM_TRY(ctx->eng->update_constants(*prms));
+}
+
+int icempm_set_current(icempm_t *ctx, const double *current_vxvy)
+{
+    ICEMPM_GUARD_CTX(ctx);
+    ICEMPM_TRY(ctx->eng->set_current(current_vxvy));
+}
+
+int icempm_step(icempm_t *ctx, int32_t nsteps, int32_t first_step)
+{
+    ICEMPM_GUARD_CTX(ctx);
+    ICEMPM_TRY(ctx->eng->step(nsteps, first_step));
+}
+
+int icempm_download_points(icempm_t *ctx, double *hssoa, uint32_t capacity, uint32_t *size)
+{
+    ICEMPM_GUARD_CTX(ctx);
+    if (!hssoa) return fail(ICEMPM_E_ARG, "hssoa is null");
+    ICEMPM_TRY(ctx->eng->download(hssoa, capacity, size));
+}
+
+int icempm_get_status(icempm_t *ctx, uint32_t *error_bits, int32_t *disabled_count)
+{
+    ICEMPM_GUARD_CTX(ctx);
+    ICEMPM_TRY(ctx->eng->status(error_bits, disabled_count));
+}
+
+int icempm_clear_force_accumulator(icempm_t *ctx)
+{
+    ICEMPM_GUARD_CTX(ctx);
+    ICEMPM_TRY(ctx->eng->clear_forces());
+}
+
+int icempm_get_boundary_forces(icempm_t *ctx, double *fxfy, int32_t elapsed_steps)
+{
+    ICEMPM_GUARD_CTX(ctx);
+    if (!fxfy) return fail(ICEMPM_E_ARG, "fxfy is null");
+    if (elapsed_steps <= 0) return fail(ICEMPM_E_ARG, "elapsed_steps must be > 0");
+    ICEMPM_TRY(ctx->eng->forces(fxfy, elapsed_steps));
+}
+
+int icempm_sort_compact(icempm_t *ctx)
+{
+    ICEMPM_GUARD_CTX(ctx);
+    ICEMPM_TRY(ctx->eng->sort_compact());
+}
+
+int icempm_timings(icempm_t *ctx, float ms[4])
+{
+    ICEMPM_GUARD_CTX(ctx);
+    if (!ms) return fail(ICEMPM_E_ARG, "ms is null");
+    ICEMPM_TRY(ctx->eng->timings(ms));
+}
+
+int icempm_phase_times(icempm_t *ctx, int32_t nsteps, float *update_ms, float *fused_ms)
+{
+    ICEMPM_GUARD_CTX(ctx);
+    if (nsteps <= 0 || !update_ms || !fused_ms) return fail(ICEMPM_E_ARG, "bad arguments");
+    ICEMPM_TRY(ctx->eng->phase_times(nsteps, update_ms, fused_ms));
+}
+
+int icempm_point_count(icempm_t *ctx, uint32_t *n)
+{
+    ICEMPM_GUARD_CTX(ctx);
+    if (!n) return fail(ICEMPM_E_ARG, "n is null");
+    *n = ctx->eng->count();
+    return ICEMPM_OK;
+}
+
+int icempm_get_stream(icempm_t *ctx, void **stream)
+{
+    ICEMPM_GUARD_CTX(ctx);
+    if (!stream) return fail(ICEMPM_E_ARG, "stream is null");
+    *stream = (void *)ctx->eng->stream();
+    return ICEMPM_OK;
+}
+
+int icempm_launch_count(icempm_t *ctx, uint64_t *count)
+{
+    ICEMPM_GUARD_CTX(ctx);
+    if (!count) return fail(ICEMPM_E_ARG, "count is null");
+    *count = ctx->eng->launches();
+    return ICEMPM_OK;
+}
+
+int icempm_fixed_point_scales(icempm_t *ctx, double *scale_mass, double *scale_momentum)
+{
+    ICEMPM_GUARD_CTX(ctx);
+    if (scale_mass) *scale_mass = ctx->eng->fixed_scale_m();
+    if (scale_momentum) *scale_momentum = ctx->eng->fixed_scale_p();
+    return ICEMPM_OK;
+}
+
+int icempm_host_register(void *ptr, size_t bytes)
+{
+    if (!ptr || !bytes) return fail(ICEMPM_E_ARG, "null or empty range");
+    cudaError_t e = cudaHostRegister(ptr, bytes, cudaHostRegisterDefault);
+    if (e != cudaSuccess) return fail(ICEMPM_E_CUDA, std::string("cudaHostRegister: ") + cudaGetErrorString(e));
+    return ICEMPM_OK;
+}
+
+int icempm_host_unregister(void *ptr)
+{
+    cudaError_t e = cudaHostUnregister(ptr);
+    if (e != cudaSuccess) return fail(ICEMPM_E_CUDA, std::string("cudaHostUnregister: ") + cudaGetErrorString(e));
+    return ICEMPM_OK;
+}
+
+int icempm_device_count(int *count)
+{
+    if (!count) return fail(ICEMPM_E_ARG, "count is null");
+    cudaError_t e = cudaGetDeviceCount(count);
+    if (e != cudaSuccess) { *count = 0; return fail(ICEMPM_E_CUDA, cudaGetErrorString(e)); }
+    return ICEMPM_OK;
+}
+
+const char *icempm_last_error(void) { return icempm::g_last_error.c_str(); }
+
+}  // extern "C"

@@ -1,0 +1,523 @@
+// engine_host.cuh -- host side of one variant of the step: device memory,
+// host<->device conversion, the step loop (CUDA graphs), locality sorting and
+// compaction.  Instantiated once per variant in engine_<variant>.cu.
+#pragma once
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+#include <algorithm>
+
+#include "engine.cuh"
+#include "engine_iface.h"
+
+namespace icempm {
+
+#define ICEMPM_CUDA(call)                                                              \
+    do {                                                                               \
+        cudaError_t e_ = (call);                                                       \
+        if (e_ != cudaSuccess) return fail(ICEMPM_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+static inline double pow2_floor(double x) { return std::ldexp(1.0, (int)std::floor(std::log2(x))); }
+
+template <class Real, class Acc>
+class EngineT final : public Engine {
+    static constexpr int BT = 256;       // points per CTA in the particle kernels
+    static constexpr int CAP = 512;      // nodes in the shared scatter tile
+    static constexpr int GRAPH_STEPS = 32;
+
+public:
+    EngineT() = default;
+    ~EngineT() override { release(); }
+
+    int init(const icempm_simparams_t &p, const uint8_t *status, const double *cur, uint32_t capacity,
+             const icempm_options_t &o) override
+    {
+        prms_ = p; opts_ = o;
+        gx_ = p.GridXTotal; gy_ = p.GridYTotal;
+        if (gx_ < 5 || gy_ < 5 || gx_ > 65535 || gy_ > 65535) return fail(ICEMPM_E_ARG, "grid size out of range");
+        if (!(p.cellsize > 0) || !(p.InitialTimeStep > 0)) return fail(ICEMPM_E_ARG, "cellsize and InitialTimeStep must be > 0");
+        G_ = (size_t)gx_ * gy_;
+        cap_ = std::max<uint32_t>(capacity, 1);
+        ICEMPM_CUDA(cudaSetDevice(o.device));
+        ICEMPM_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+        ICEMPM_CUDA(cudaEventCreate(&ev0_));
+        ICEMPM_CUDA(cudaEventCreate(&ev1_));
+        ICEMPM_CUDA(cudaEventCreate(&evs_[0]));
+        ICEMPM_CUDA(cudaEventCreate(&evs_[1]));
+        ICEMPM_CUDA(cudaEventCreate(&evs_[2]));
+        // points, two parities for the sort gather
+        const size_t nc = ((size_t)cap_ + 255) / 256 * 256;
+        const size_t per = nc * (3 * sizeof(V4<Real>) + 2 * sizeof(V2<Real>) + sizeof(uint2) + 2 * sizeof(uint32_t) + sizeof(double));
+        ICEMPM_CUDA(cudaMalloc(&pts_mem_, 2 * per));
+        for (int par = 0; par < 2; par++) {
+            char *b = (char *)pts_mem_ + par * per;
+            auto take = [&](size_t bytes) { char *r = b; b += bytes; return r; };
+            Pts<Real> &P = pts_[par];
+            P.A = (V4<Real> *)take(nc * sizeof(V4<Real>));
+            P.H = (V4<Real> *)take(nc * sizeof(V4<Real>));
+            P.C = (V4<Real> *)take(nc * sizeof(V4<Real>));
+            P.V = (V2<Real> *)take(nc * sizeof(V2<Real>));
+            P.PQ = (V2<Real> *)take(nc * sizeof(V2<Real>));
+            P.K = (uint2 *)take(nc * sizeof(uint2));
+            P.thick64 = (double *)take(nc * sizeof(double));
+            P.slot = (uint32_t *)take(nc * sizeof(uint32_t));
+            P.pid = (uint32_t *)take(nc * sizeof(uint32_t));
+        }
+        // grid
+        ICEMPM_CUDA(cudaMalloc(&acc_, G_ * sizeof(Acc4<Acc>)));
+        ICEMPM_CUDA(cudaMalloc(&vel_, G_ * sizeof(V2<Real>)));
+        ICEMPM_CUDA(cudaMalloc(&cur_, G_ * sizeof(V2<Real>)));
+        ICEMPM_CUDA(cudaMalloc(&status_, G_));
+        ICEMPM_CUDA(cudaMalloc(&force_, G_ * sizeof(double2)));
+        ICEMPM_CUDA(cudaMalloc(&st_, sizeof(DevStatus)));
+        ICEMPM_CUDA(cudaMemsetAsync(acc_, 0, G_ * sizeof(Acc4<Acc>), stream_));
+        ICEMPM_CUDA(cudaMemsetAsync(vel_, 0, G_ * sizeof(V2<Real>), stream_));
+        ICEMPM_CUDA(cudaMemsetAsync(force_, 0, G_ * sizeof(double2), stream_));
+        ICEMPM_CUDA(cudaMemsetAsync(st_, 0, sizeof(DevStatus), stream_));
+        ICEMPM_CUDA(cudaMemcpyAsync(status_, status, G_, cudaMemcpyHostToDevice, stream_));
+        ICEMPM_CUDA(cudaStreamSynchronize(stream_));
+        int rc = set_current(cur);
+        if (rc) return rc;
+        // sort buffers
+        ICEMPM_CUDA(cudaMalloc(&keys_[0], nc * sizeof(uint64_t)));
+        ICEMPM_CUDA(cudaMalloc(&keys_[1], nc * sizeof(uint64_t)));
+        ICEMPM_CUDA(cudaMalloc(&vals_[0], nc * sizeof(uint32_t)));
+        ICEMPM_CUDA(cudaMalloc(&vals_[1], nc * sizeof(uint32_t)));
+        size_t t32 = 0, t64 = 0;
+        ICEMPM_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, t32, (uint32_t *)nullptr, (uint32_t *)nullptr,
+                                                    (uint32_t *)nullptr, (uint32_t *)nullptr, (int)nc, 0, 32, stream_));
+        ICEMPM_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, t64, (uint64_t *)nullptr, (uint64_t *)nullptr,
+                                                    (uint32_t *)nullptr, (uint32_t *)nullptr, (int)nc, 0, 64, stream_));
+        sort_tmp_bytes_ = std::max(t32, t64);
+        ICEMPM_CUDA(cudaMalloc(&sort_tmp_, sort_tmp_bytes_));
+        tile_.tx = 8; tile_.ty = 8;
+        if (opts_.block_threads == 128) { tile_.tx = 8; tile_.ty = 4; }
+        tile_.ntiles_y = (gy_ + tile_.ty - 1) / tile_.ty;
+        return set_params(p, 1.0);
+    }
+
+    int set_params(const icempm_simparams_t &p, double max_thickness) override
+    {
+        prms_ = p;
+        if (max_thickness > 0) max_thick_ = max_thickness;
+        KParams<Real> &k = kp_;
+        k.gx = gx_; k.gy = gy_;
+        k.update_every = p.UpdateEveryNthStep;
+        k.forcing = opts_.forcing; k.wind_kind = opts_.wind_kind;
+        k.h = Real(p.cellsize); k.h_inv = Real(p.cellsize_inv);
+        k.dt = Real(p.InitialTimeStep);
+        k.dt_h_inv = Real(p.InitialTimeStep * p.cellsize_inv);
+        k.four_h_inv = Real(4.0 * p.cellsize_inv);
+        k.vmax2_01 = Real(p.vmax * p.vmax * 0.1);
+        k.particle_mass = Real(p.ParticleMass);
+        k.dt_vol_Dpinv = Real(p.dt_vol_Dpinv);
+        k.particle_volume = Real(p.ParticleVolume);
+        k.dt_d = p.InitialTimeStep;
+        k.kL = p.waterDragEffectiveLinear * p.InitialTimeStep;
+        k.kQ = p.waterDragEffectiveQuadratic * p.InitialTimeStep;
+        const double mref = std::max(p.ParticleMass * max_thick_, 1e-30);
+        k.scale_m = pow2_floor(std::ldexp(1.0, 62) / (4096.0 * mref));
+        k.scale_p = k.scale_m / 16.0;
+        k.scale_a = pow2_floor(std::ldexp(1.0, 62) / (4096.0 * std::max(p.ParticleVolume, 1e-30)));
+        k.inv_scale_m = 1.0 / k.scale_m; k.inv_scale_p = 1.0 / k.scale_p; k.inv_scale_a = 1.0 / k.scale_a;
+        k.lim_m = std::ldexp(1.0, 52) / k.scale_m;
+        k.lim_p = std::ldexp(1.0, 52) / k.scale_p;
+        k.rho_w_cd_dt = opts_.water_density * opts_.water_drag_coeff * p.InitialTimeStep;
+        k.rho_a_ca_dt = opts_.air_density * opts_.air_drag_coeff * p.InitialTimeStep;
+        k.wind_u = opts_.wind_u; k.wind_v = opts_.wind_v;
+        k.wind_cx = opts_.wind_cx; k.wind_cy = opts_.wind_cy;
+        k.wind_vmax = opts_.wind_vmax; k.wind_radius = opts_.wind_radius;
+        Material &m = k.mat;
+        m.mu = p.mu; m.kappa = p.kappa; m.DP_threshold_p = p.DP_threshold_p;
+        m.pmax = p.IceCompressiveStrength; m.pmin = -p.IceTensileStrength;
+        m.qmax = p.IceShearStrength; m.pmin2 = -p.IceTensileStrength2;
+        m.beta = p.IceTensileStrength / p.IceCompressiveStrength;
+        m.M_sq = (4. * m.qmax * m.qmax * (1. + 2. * m.beta)) / ((m.pmax - m.pmin) * (m.pmax - m.pmin));
+        m.tan_phi = std::tan(p.DP_phi * ICEMPM_PI / 180);
+        m.ridge_coeff_g_rho = p.RidgeFormationCoeff * ICEMPM_GRAVITY * p.IceDensity;
+        primed_ = false;
+        invalidate_graphs();
+        return 0;
+    }
+
+    int set_current(const double *cur) override
+    {
+        std::vector<V2<Real>> h(G_);
+        for (size_t i = 0; i < G_; i++) {
+            h[i].x = cur ? Real(cur[i]) : Real(0);
+            h[i].y = cur ? Real(cur[G_ + i]) : Real(0);
+        }
+        ICEMPM_CUDA(cudaMemcpyAsync(cur_, h.data(), G_ * sizeof(V2<Real>), cudaMemcpyHostToDevice, stream_));
+        ICEMPM_CUDA(cudaStreamSynchronize(stream_));
+        return 0;
+    }
+
+    int ensure_stage()
+    {
+        if (stage_) return 0;
+        ICEMPM_CUDA(cudaMalloc(&stage_, (size_t)ICEMPM_N_PTS_ARRAYS * cap_ * sizeof(double)));
+        return 0;
+    }
+
+    int upload(const double *hssoa, uint32_t host_cap, uint32_t n, int32_t disabled) override
+    {
+        if (n > cap_) return fail(ICEMPM_E_CAPACITY, "point count exceeds the context capacity");
+        if (n > host_cap) return fail(ICEMPM_E_ARG, "size exceeds the host buffer capacity");
+        int rc = ensure_stage();
+        if (rc) return rc;
+        if (n > 0) {
+            ICEMPM_CUDA(cudaMemcpy2DAsync(stage_, (size_t)n * sizeof(double), hssoa, (size_t)host_cap * sizeof(double),
+                                          (size_t)n * sizeof(double), ICEMPM_N_PTS_ARRAYS, cudaMemcpyHostToDevice, stream_));
+            k_upload<Real><<<(n + 255) / 256, 256, 0, stream_>>>(stage_, n, (int)n, pts_[par_]);
+            ICEMPM_CUDA(cudaGetLastError());
+            launches_++;
+        }
+        n_ = n;
+        double mt = 0;
+        for (uint32_t i = 0; i < n; i++) mt = std::max(mt, std::fabs(hssoa[(size_t)18 * host_cap + i]));
+        set_params(prms_, mt > 0 ? mt : 1.0);
+        DevStatus s{};
+        s.disabled = disabled;
+        ICEMPM_CUDA(cudaMemcpyAsync(&st_->disabled, &s.disabled, sizeof(int32_t), cudaMemcpyHostToDevice, stream_));
+        ICEMPM_CUDA(cudaStreamSynchronize(stream_));
+        steps_since_sort_ = 0;
+        if (n_ > 0) {
+            rc = locality_sort();
+            if (rc) return rc;
+        }
+        return 0;
+    }
+
+    int download(double *hssoa, uint32_t host_cap, uint32_t *size) override
+    {
+        if (n_ > host_cap) return fail(ICEMPM_E_CAPACITY, "host buffer capacity is smaller than the point count");
+        int rc = ensure_stage();
+        if (rc) return rc;
+        if (n_ > 0) {
+            k_download<Real><<<(n_ + 255) / 256, 256, 0, stream_>>>(pts_[par_], (int)n_, stage_, n_);
+            ICEMPM_CUDA(cudaGetLastError());
+            launches_++;
+            ICEMPM_CUDA(cudaMemcpy2DAsync(hssoa, (size_t)host_cap * sizeof(double), stage_, (size_t)n_ * sizeof(double),
+                                          (size_t)n_ * sizeof(double), ICEMPM_N_PTS_ARRAYS, cudaMemcpyDeviceToHost, stream_));
+        }
+        ICEMPM_CUDA(cudaStreamSynchronize(stream_));
+        if (size) *size = n_;
+        return 0;
+    }
+
+    int update_constants(const icempm_simparams_t &p) override
+    {
+        const uint32_t zero = 0;
+        ICEMPM_CUDA(cudaMemcpyAsync(&st_->err, &zero, sizeof(zero), cudaMemcpyHostToDevice, stream_));
+        ICEMPM_CUDA(cudaStreamSynchronize(stream_));
+        return set_params(p, -1.0);
+    }
+
+    // ---------------------------------------------------------------- step
+    void launch_update()
+    {
+        const unsigned nb = (unsigned)((G_ + 255) / 256);
+        if (opts_.forcing == ICEMPM_FORCING_EXTENDED)
+            k_grid_update<Real, Acc, true><<<nb, 256, 0, stream_>>>(kp_, grid(), st_, (long long)G_);
+        else
+            k_grid_update<Real, Acc, false><<<nb, 256, 0, stream_>>>(kp_, grid(), st_, (long long)G_);
+        launches_++;
+    }
+
+    template <int NCH, bool WR> void launch_fused_t()
+    {
+        const unsigned nb = (n_ + BT - 1) / BT;
+        k_g2p_p2g<Real, Acc, NCH, BT, CAP, WR><<<nb, BT, 0, stream_>>>(kp_, pts_[par_], grid(), st_, (int)n_);
+    }
+    void launch_fused()
+    {
+        const bool ext = opts_.forcing == ICEMPM_FORCING_EXTENDED;
+        const bool wr = opts_.warp_reduce != 0;
+        if (ext) { if (wr) launch_fused_t<4, true>(); else launch_fused_t<4, false>(); }
+        else { if (wr) launch_fused_t<3, true>(); else launch_fused_t<3, false>(); }
+        launches_++;
+    }
+    template <int NCH, bool WR> void launch_p2g_t()
+    {
+        const unsigned nb = (n_ + BT - 1) / BT;
+        k_p2g<Real, Acc, NCH, BT, CAP, WR><<<nb, BT, 0, stream_>>>(kp_, pts_[par_], grid(), st_, (int)n_);
+    }
+    int prime()
+    {
+        ICEMPM_CUDA(cudaMemsetAsync(acc_, 0, G_ * sizeof(Acc4<Acc>), stream_));
+        if (n_ > 0) {
+            const bool ext = opts_.forcing == ICEMPM_FORCING_EXTENDED;
+            const bool wr = opts_.warp_reduce != 0;
+            if (ext) { if (wr) launch_p2g_t<4, true>(); else launch_p2g_t<4, false>(); }
+            else { if (wr) launch_p2g_t<3, true>(); else launch_p2g_t<3, false>(); }
+            launches_++;
+            ICEMPM_CUDA(cudaGetLastError());
+        }
+        primed_ = true;
+        return 0;
+    }
+
+    int run_chunk_direct(int k)
+    {
+        for (int s = 0; s < k; s++) {
+            launch_update();
+            if (n_ > 0) launch_fused();
+        }
+        ICEMPM_CUDA(cudaGetLastError());
+        return 0;
+    }
+
+    int run_chunk_graph()
+    {
+        if (!graph_exec_ || graph_n_ != n_ || graph_par_ != par_) {
+            invalidate_graphs();
+            cudaGraph_t g;
+            ICEMPM_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+            const uint64_t before = launches_;
+            for (int s = 0; s < GRAPH_STEPS; s++) {
+                launch_update();
+                if (n_ > 0) launch_fused();
+            }
+            graph_launches_ = launches_ - before;
+            launches_ = before;
+            cudaError_t e = cudaStreamEndCapture(stream_, &g);
+            if (e != cudaSuccess) return fail(ICEMPM_E_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+            e = cudaGraphInstantiate(&graph_exec_, g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) { graph_exec_ = nullptr; return fail(ICEMPM_E_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e)); }
+            graph_n_ = n_; graph_par_ = par_;
+        }
+        ICEMPM_CUDA(cudaGraphLaunch(graph_exec_, stream_));
+        launches_ += graph_launches_;
+        return 0;
+    }
+
+    int step(int nsteps, int first_step) override
+    {
+        if (nsteps < 0) return fail(ICEMPM_E_ARG, "nsteps < 0");
+        ICEMPM_CUDA(cudaEventRecord(ev0_, stream_));
+        k_set_step<<<1, 1, 0, stream_>>>(st_, first_step, 1);
+        launches_++;
+        int rc = 0;
+        if (!primed_) { rc = prime(); if (rc) return rc; }
+        float sort_ms = 0;
+        int remaining = nsteps;
+        while (remaining > 0) {
+            if (opts_.sort_every > 0 && steps_since_sort_ >= opts_.sort_every && n_ > 0) {
+                ICEMPM_CUDA(cudaEventRecord(evs_[0], stream_));
+                rc = locality_sort();
+                if (rc) return rc;
+                ICEMPM_CUDA(cudaEventRecord(evs_[1], stream_));
+                ICEMPM_CUDA(cudaEventSynchronize(evs_[1]));
+                float ms = 0;
+                cudaEventElapsedTime(&ms, evs_[0], evs_[1]);
+                sort_ms += ms;
+            }
+            int chunk = remaining;
+            if (opts_.sort_every > 0) chunk = std::min(chunk, std::max(1, opts_.sort_every - steps_since_sort_));
+            if (opts_.use_graphs && chunk >= GRAPH_STEPS) {
+                chunk = GRAPH_STEPS;
+                rc = run_chunk_graph();
+            } else {
+                rc = run_chunk_direct(chunk);
+            }
+            if (rc) return rc;
+            remaining -= chunk;
+            steps_since_sort_ += chunk;
+        }
+        ICEMPM_CUDA(cudaEventRecord(ev1_, stream_));
+        last_sort_ms_ = sort_ms;
+        timed_ = true;
+        return 0;
+    }
+
+    // Device time between the event pair around the last icempm_step or
+    // icempm_phase_times call, and the locality-sort time inside it.
+    int timings(float ms[4]) override
+    {
+        ms[0] = ms[1] = ms[2] = ms[3] = 0;
+        if (timed_) {
+            ICEMPM_CUDA(cudaEventSynchronize(ev1_));
+            ICEMPM_CUDA(cudaEventElapsedTime(&ms[0], ev0_, ev1_));
+        }
+        ms[3] = last_sort_ms_;
+        return 0;
+    }
+
+    int phase_times(int nsteps, float *update_ms, float *fused_ms) override
+    {
+        // time nsteps steps launched directly, accumulating per-kernel event pairs
+        if (!primed_) { int rc = prime(); if (rc) return rc; }
+        std::vector<cudaEvent_t> ev(3 * nsteps);
+        for (auto &e : ev) ICEMPM_CUDA(cudaEventCreate(&e));
+        ICEMPM_CUDA(cudaEventRecord(ev0_, stream_));
+        for (int s = 0; s < nsteps; s++) {
+            cudaEventRecord(ev[3 * s], stream_);
+            launch_update();
+            cudaEventRecord(ev[3 * s + 1], stream_);
+            if (n_ > 0) launch_fused();
+            cudaEventRecord(ev[3 * s + 2], stream_);
+        }
+        ICEMPM_CUDA(cudaEventRecord(ev1_, stream_));
+        ICEMPM_CUDA(cudaGetLastError());
+        ICEMPM_CUDA(cudaStreamSynchronize(stream_));
+        timed_ = true;
+        last_sort_ms_ = 0;
+        float u = 0, f = 0;
+        for (int s = 0; s < nsteps; s++) {
+            float a = 0, b = 0;
+            cudaEventElapsedTime(&a, ev[3 * s], ev[3 * s + 1]);
+            cudaEventElapsedTime(&b, ev[3 * s + 1], ev[3 * s + 2]);
+            u += a; f += b;
+        }
+        for (auto &e : ev) cudaEventDestroy(e);
+        *update_ms = u; *fused_ms = f;
+        steps_since_sort_ += nsteps;
+        return 0;
+    }
+
+    int status(uint32_t *err, int32_t *dis) override
+    {
+        DevStatus s;
+        ICEMPM_CUDA(cudaMemcpyAsync(&s, st_, sizeof(s), cudaMemcpyDeviceToHost, stream_));
+        ICEMPM_CUDA(cudaStreamSynchronize(stream_));
+        if (err) *err = s.err;
+        if (dis) *dis = s.disabled;
+        return 0;
+    }
+
+    int clear_forces() override
+    {
+        ICEMPM_CUDA(cudaMemsetAsync(force_, 0, G_ * sizeof(double2), stream_));
+        return 0;
+    }
+
+    int forces(double *fxfy, int elapsed) override
+    {
+        std::vector<double2> h(G_);
+        ICEMPM_CUDA(cudaMemcpyAsync(h.data(), force_, G_ * sizeof(double2), cudaMemcpyDeviceToHost, stream_));
+        ICEMPM_CUDA(cudaStreamSynchronize(stream_));
+        const double div = (double)elapsed * prms_.InitialTimeStep;
+        for (size_t i = 0; i < G_; i++) {
+            fxfy[i] = h[i].x / div;
+            fxfy[G_ + i] = h[i].y / div;
+        }
+        return 0;
+    }
+
+    // Sort by the tiled locality key into the other parity (host slots unchanged).
+    int locality_sort()
+    {
+        if (n_ == 0) return 0;
+        const unsigned nb = (n_ + 255) / 256;
+        uint32_t *k32in = (uint32_t *)keys_[0], *k32out = (uint32_t *)keys_[1];
+        k_keys_tiled<<<nb, 256, 0, stream_>>>(pts_[par_].K, (int)n_, tile_, k32in, vals_[0]);
+        launches_++;
+        size_t tb = sort_tmp_bytes_;
+        ICEMPM_CUDA(cub::DeviceRadixSort::SortPairs(sort_tmp_, tb, k32in, k32out, vals_[0], vals_[1], (int)n_, 0, 32, stream_));
+        launches_ += 4;
+        k_gather<Real><<<nb, 256, 0, stream_>>>(pts_[par_], pts_[1 - par_], vals_[1], (int)n_, 0);
+        launches_++;
+        ICEMPM_CUDA(cudaGetLastError());
+        par_ = 1 - par_;
+        steps_since_sort_ = 0;
+        invalidate_graphs();
+        return 0;
+    }
+
+    // RemoveDisabledAndSort (host_side_soa.cpp:36-47) on the device.
+    int sort_compact() override
+    {
+        if (n_ > 0) {
+            const unsigned nb = (n_ + 255) / 256;
+            k_keys_reference<<<nb, 256, 0, stream_>>>(pts_[par_].K, pts_[par_].slot, (int)n_, gy_, keys_[0], vals_[0]);
+            launches_++;
+            size_t tb = sort_tmp_bytes_;
+            ICEMPM_CUDA(cub::DeviceRadixSort::SortPairs(sort_tmp_, tb, keys_[0], keys_[1], vals_[0], vals_[1], (int)n_, 0, 64, stream_));
+            launches_ += 4;
+            k_gather<Real><<<nb, 256, 0, stream_>>>(pts_[par_], pts_[1 - par_], vals_[1], (int)n_, 1);
+            k_count_active<<<nb, 256, 0, stream_>>>(keys_[1], (int)n_, st_);
+            launches_ += 2;
+            ICEMPM_CUDA(cudaGetLastError());
+            par_ = 1 - par_;
+            DevStatus s;
+            ICEMPM_CUDA(cudaMemcpyAsync(&s, st_, sizeof(s), cudaMemcpyDeviceToHost, stream_));
+            ICEMPM_CUDA(cudaStreamSynchronize(stream_));
+            n_ = (uint32_t)s.n_active;
+        }
+        const int32_t zero = 0;
+        ICEMPM_CUDA(cudaMemcpyAsync(&st_->disabled, &zero, sizeof(zero), cudaMemcpyHostToDevice, stream_));
+        ICEMPM_CUDA(cudaStreamSynchronize(stream_));
+        primed_ = false;
+        invalidate_graphs();
+        return locality_sort();
+    }
+
+    uint32_t count() const override { return n_; }
+    cudaStream_t stream() const override { return stream_; }
+    uint64_t launches() const override { return launches_; }
+    double fixed_scale_m() const override { return kp_.scale_m; }
+    double fixed_scale_p() const override { return kp_.scale_p; }
+
+private:
+    Grid<Real, Acc> grid() const
+    {
+        Grid<Real, Acc> g;
+        g.acc = acc_; g.vel = vel_; g.cur = cur_; g.status = status_; g.force = force_;
+        return g;
+    }
+    void invalidate_graphs()
+    {
+        if (graph_exec_) { cudaGraphExecDestroy(graph_exec_); graph_exec_ = nullptr; }
+    }
+    void release()
+    {
+        if (stream_) cudaStreamSynchronize(stream_);
+        invalidate_graphs();
+        cudaFree(pts_mem_); cudaFree(acc_); cudaFree(vel_); cudaFree(cur_); cudaFree(status_);
+        cudaFree(force_); cudaFree(st_); cudaFree(stage_); cudaFree(keys_[0]); cudaFree(keys_[1]);
+        cudaFree(vals_[0]); cudaFree(vals_[1]); cudaFree(sort_tmp_);
+        if (ev0_) cudaEventDestroy(ev0_);
+        if (ev1_) cudaEventDestroy(ev1_);
+        for (auto &e : evs_) if (e) cudaEventDestroy(e);
+        if (stream_) cudaStreamDestroy(stream_);
+        stream_ = nullptr;
+    }
+
+    icempm_simparams_t prms_{};
+    icempm_options_t opts_{};
+    int gx_ = 0, gy_ = 0;
+    size_t G_ = 0;
+    uint32_t cap_ = 0, n_ = 0;
+    double max_thick_ = 1.0;
+    cudaStream_t stream_ = nullptr;
+    cudaEvent_t ev0_ = nullptr, ev1_ = nullptr, evs_[3] = {nullptr, nullptr, nullptr};
+    void *pts_mem_ = nullptr;
+    Pts<Real> pts_[2]{};
+    int par_ = 0;
+    Acc4<Acc> *acc_ = nullptr;
+    V2<Real> *vel_ = nullptr, *cur_ = nullptr;
+    uint8_t *status_ = nullptr;
+    double2 *force_ = nullptr;
+    DevStatus *st_ = nullptr;
+    double *stage_ = nullptr;
+    uint64_t *keys_[2] = {nullptr, nullptr};
+    uint32_t *vals_[2] = {nullptr, nullptr};
+    void *sort_tmp_ = nullptr;
+    size_t sort_tmp_bytes_ = 0;
+    TileKey tile_{8, 8, 1};
+    KParams<Real> kp_{};
+    bool primed_ = false, timed_ = false;
+    int steps_since_sort_ = 0;
+    float last_sort_ms_ = 0;
+    cudaGraphExec_t graph_exec_ = nullptr;
+    uint32_t graph_n_ = 0;
+    int graph_par_ = -1;
+    uint64_t graph_launches_ = 0;
+    uint64_t launches_ = 0;
+};
+
+}  // namespace icempm

@@ -1,0 +1,42 @@
+// engine_iface.h -- variant-independent interface between the C ABI (capi.cu)
+// and the per-variant engines (engine_<variant>.cu).
+#pragma once
+#include <cstdint>
+#include <string>
+#include <cuda_runtime.h>
+#include "../../include/icempm.h"
+
+namespace icempm {
+
+// Records `msg` as the calling thread's last error and returns `code`.
+int fail(int code, const std::string &msg);
+
+class Engine {
+public:
+    virtual ~Engine() {}
+    virtual int init(const icempm_simparams_t &p, const uint8_t *status, const double *cur, uint32_t capacity,
+                     const icempm_options_t &o) = 0;
+    virtual int set_params(const icempm_simparams_t &p, double max_thickness) = 0;
+    virtual int set_current(const double *cur) = 0;
+    virtual int upload(const double *hssoa, uint32_t host_cap, uint32_t n, int32_t disabled) = 0;
+    virtual int download(double *hssoa, uint32_t host_cap, uint32_t *size) = 0;
+    virtual int update_constants(const icempm_simparams_t &p) = 0;
+    virtual int step(int nsteps, int first_step) = 0;
+    virtual int timings(float ms[4]) = 0;
+    virtual int phase_times(int nsteps, float *update_ms, float *fused_ms) = 0;
+    virtual int status(uint32_t *err, int32_t *dis) = 0;
+    virtual int clear_forces() = 0;
+    virtual int forces(double *fxfy, int elapsed) = 0;
+    virtual int sort_compact() = 0;
+    virtual uint32_t count() const = 0;
+    virtual cudaStream_t stream() const = 0;
+    virtual uint64_t launches() const = 0;
+    virtual double fixed_scale_m() const = 0;
+    virtual double fixed_scale_p() const = 0;
+};
+
+Engine *make_engine_fixed();
+Engine *make_engine_fp32();
+Engine *make_engine_fp64();
+
+}  // namespace icempm

@@ -26,6 +26,12 @@
 #include <stdbool.h>
 #endif
 
+#if defined(__GNUC__)
+#define ICEMPM_API __attribute__((visibility("default")))
+#else
+#define ICEMPM_API
+#endif
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -159,7 +165,7 @@ typedef struct icempm_options {
 typedef struct icempm_context icempm_t;
 
 /* Fill `opts` with the defaults (fixed-point variant, compat forcing). */
-void icempm_default_options(icempm_options_t *opts);
+ICEMPM_API void icempm_default_options(icempm_options_t *opts);
 
 /* Create a context for one scene on one GPU.
  * Replaces GPU_Implementation5::initialize + GPU_Partition::allocate +
@@ -170,75 +176,94 @@ void icempm_default_options(icempm_options_t *opts);
  *   current_vxvy  : 2*GridX*GridY doubles (vx block then vy block) or NULL (zero current)
  *   capacity      : maximum number of points the device arrays hold
  *   opts          : NULL for defaults */
-int icempm_create(const icempm_simparams_t *prms, const uint8_t *grid_status,
+ICEMPM_API int icempm_create(const icempm_simparams_t *prms, const uint8_t *grid_status,
                   const double *current_vxvy, uint32_t capacity,
                   const icempm_options_t *opts, icempm_t **out);
 
 /* Destroy a context and free its device memory (GPU_Partition::~GPU_Partition,
  * gpu_partition.cpp:214-232). NULL is accepted. */
-int icempm_destroy(icempm_t *ctx);
+ICEMPM_API int icempm_destroy(icempm_t *ctx);
 
 /* Upload `size` points from a reference-layout HSSOA buffer (19 rows of
  * `capacity` doubles).  Replaces GPU_Partition::transfer_points_from_soa_to_device
  * (gpu_partition.cpp:81-106).  disabled_count seeds the device counter. */
-int icempm_upload_points(icempm_t *ctx, const double *hssoa, uint32_t capacity,
+ICEMPM_API int icempm_upload_points(icempm_t *ctx, const double *hssoa, uint32_t capacity,
                          uint32_t size, int32_t disabled_count);
 
 /* Re-read SimParams (GPU_Partition::update_constants, gpu_partition.cpp:140-170).
  * Also clears the device error word as the reference does. */
-int icempm_update_constants(icempm_t *ctx, const icempm_simparams_t *prms);
+ICEMPM_API int icempm_update_constants(icempm_t *ctx, const icempm_simparams_t *prms);
 
 /* Replace the current field (GPU_Partition::update_current_field,
  * gpu_partition.cpp:174-196): 2*GridX*GridY doubles, vx block then vy block. */
-int icempm_set_current(icempm_t *ctx, const double *current_vxvy);
+ICEMPM_API int icempm_set_current(icempm_t *ctx, const double *current_vxvy);
 
 /* Advance `nsteps` sub-steps starting at step index `first_step`.  Step k runs
  * reset_grid, p2g, update_nodes(t = dt*k rounded to float) and
  * g2p(recordPQ = (k % UpdateEveryNthStep == 0)), exactly as the loop in
  * Model::Step (model.cpp:18-39).  Asynchronous: returns after enqueueing. */
-int icempm_step(icempm_t *ctx, int32_t nsteps, int32_t first_step);
+ICEMPM_API int icempm_step(icempm_t *ctx, int32_t nsteps, int32_t first_step);
 
 /* Download all points into a reference-layout HSSOA buffer, in the slot order
  * of the last upload (or of the last icempm_sort_compact).  Replaces
  * GPU_Partition::transfer_from_device's point part (gpu_partition.cpp:17-38).
  * Synchronises the stream.  *size receives the number of points. */
-int icempm_download_points(icempm_t *ctx, double *hssoa, uint32_t capacity, uint32_t *size);
+ICEMPM_API int icempm_download_points(icempm_t *ctx, double *hssoa, uint32_t capacity, uint32_t *size);
 
 /* Fetch the device error bitmask and disabled-point counter
  * (gpu_partition.cpp:40-48).  Synchronises the stream. */
-int icempm_get_status(icempm_t *ctx, uint32_t *error_bits, int32_t *disabled_count);
+ICEMPM_API int icempm_get_status(icempm_t *ctx, uint32_t *error_bits, int32_t *disabled_count);
 
 /* Zero the boundary-force accumulators (GPU_Partition::clear_force_accumulator,
  * gpu_partition.cpp:310-319). */
-int icempm_clear_force_accumulator(icempm_t *ctx);
+ICEMPM_API int icempm_clear_force_accumulator(icempm_t *ctx);
 
 /* Download the accumulated boundary forces into fxfy (2*GridX*GridY doubles,
  * fx block then fy block) divided by elapsed_steps*dt, as
  * GPU_Implementation5::transfer_from_device does (gpu_implementation5.cpp:188-224). */
-int icempm_get_boundary_forces(icempm_t *ctx, double *fxfy, int32_t elapsed_steps);
+ICEMPM_API int icempm_get_boundary_forces(icempm_t *ctx, double *fxfy, int32_t elapsed_steps);
 
 /* Remove disabled points and sort the rest by cell index x*GridY+y, on the
  * device.  Same result as HostSideSOA::RemoveDisabledAndSort followed by a
  * re-upload (host_side_soa.cpp:36-47, model.cpp:63-72); ties keep their
  * previous relative order.  Resets the disabled counter to 0. */
-int icempm_sort_compact(icempm_t *ctx);
+ICEMPM_API int icempm_sort_compact(icempm_t *ctx);
 
 /* Device time of the last icempm_step call, in ms: [0] total, [1] grid
  * update kernels, [2] fused G2P+P2G kernels, [3] locality re-sorts.
  * Synchronises the stream. (GPU_Partition::record_timings, gpu_partition.cpp:370-436) */
-int icempm_timings(icempm_t *ctx, float ms[4]);
+ICEMPM_API int icempm_timings(icempm_t *ctx, float ms[4]);
+
+/* Run `nsteps` further sub-steps launched one by one (no CUDA graph) with a
+ * CUDA event pair around every kernel, and report the summed device time of
+ * the grid-update kernels and of the fused G2P+P2G kernels.  Continues from
+ * the device step counter; used for per-kernel profiling. (No reference
+ * counterpart beyond the phase columns of GPU_Partition::record_timings.) */
+ICEMPM_API int icempm_phase_times(icempm_t *ctx, int32_t nsteps, float *update_ms, float *fused_ms);
+
+/* Fixed-point scales of the P2G accumulators (value * scale -> int64) of the
+ * FIXED variant.  No reference counterpart. */
+ICEMPM_API int icempm_fixed_point_scales(icempm_t *ctx, double *scale_mass, double *scale_momentum);
+
+/* Page-lock a caller-owned host range for asynchronous copies
+ * (cudaHostRegister) and release it again.  No reference counterpart. */
+ICEMPM_API int icempm_host_register(void *ptr, size_t bytes);
+ICEMPM_API int icempm_host_unregister(void *ptr);
+
+/* Number of visible CUDA devices (0 with a negative return when none). */
+ICEMPM_API int icempm_device_count(int *count);
 
 /* Number of points currently on the device (including disabled ones). */
-int icempm_point_count(icempm_t *ctx, uint32_t *n);
+ICEMPM_API int icempm_point_count(icempm_t *ctx, uint32_t *n);
 
 /* CUDA stream the context enqueues on (cudaStream_t), for event timing. */
-int icempm_get_stream(icempm_t *ctx, void **stream);
+ICEMPM_API int icempm_get_stream(icempm_t *ctx, void **stream);
 
 /* Number of kernel launches this context has enqueued since creation. */
-int icempm_launch_count(icempm_t *ctx, uint64_t *count);
+ICEMPM_API int icempm_launch_count(icempm_t *ctx, uint64_t *count);
 
 /* Message of the last failing call on this thread ("" if none). */
-const char *icempm_last_error(void);
+ICEMPM_API const char *icempm_last_error(void);
 
 #ifdef __cplusplus
 }

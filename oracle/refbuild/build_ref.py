@@ -40,7 +40,7 @@ def build(force: bool = False) -> str:
     if not force and os.path.exists(LIB) and all(os.path.getmtime(LIB) >= os.path.getmtime(d) for d in deps):
         return LIB
     os.makedirs(OUT_DIR, exist_ok=True)
-    cmd = ["g++", "-std=c++20", "-O2", "-ffp-contract=off", "-fPIC", "-shared", "-w",
+    cmd = ["g++", "-std=c++20", "-O2", "-fopenmp", "-ffp-contract=off", "-fPIC", "-shared", "-w",
            "-I", os.path.join(HERE, "stubs"),
            "-I", sim, "-I", os.path.join(sim, "hssoa"),
            "-I", os.path.join(REF, "External"),
@@ -79,6 +79,7 @@ def load():
         L.ref_run_steps.restype = C.c_uint32
         L.ref_remove_disabled_and_sort.argtypes = [dp, C.c_uint, C.c_uint, C.c_int]
         L.ref_remove_disabled_and_sort.restype = C.c_uint
+        L.ref_num_threads.restype = C.c_int
         _lib = L
     return _lib
 

@@ -3,17 +3,21 @@
  *   parameters_sim.cpp, hssoa/host_side_soa.cpp, hssoa/proxypoint2d.cpp
  * compiled unmodified, where they lie, by oracle/refbuild/build_ref.py, with
  * the stand-in headers in stubs/.  The three __global__ kernels run as plain
- * functions, once per (block, thread) in index order, so the P2G "atomics"
- * are applied in point-index order.  TEST INFRASTRUCTURE ONLY: it pins the
+ * functions, once per (block, thread); P2G runs serially in index order, so
+ * its "atomics" are applied in point-index order; the grid update and G2P
+ * run their blocks in parallel.  TEST INFRASTRUCTURE ONLY: it pins the
  * oracle restatement (oracle/icempm_oracle.c) to the reference code. */
 #include <cstddef>
 #include <cstdint>
 #include <cstring>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
 
 #include "parameters_sim.h"
 #include "helper_math.cuh"
 
-ref_dim3 blockIdx, threadIdx, blockDim;
+thread_local ref_dim3 blockIdx, threadIdx, blockDim;
 
 /* prototypes of the kernel helpers, same signatures as gpu_partition.h:28-59 */
 __device__ void svd2x2(const PointMatrix2r &mA, PointMatrix2r &mU, PointVector2r &mS, PointMatrix2r &mV);
@@ -41,11 +45,28 @@ __device__ void CalculateWeightCoeffs(const PointVector2r &pos, PointArray2r ww[
 #include "kernels.cuh"
 #include "host_side_soa.h"
 
+/* Serial launch: blocks and threads in index order (used for P2G, whose
+ * floating-point atomics are emulated as plain adds). */
 template <class K> static void emulate_launch(size_t nthreads, int tpb, K kernel)
 {
     const size_t nblocks = (nthreads + tpb - 1) / tpb;
     blockDim.x = tpb;
     for (size_t b = 0; b < nblocks; b++) {
+        blockIdx.x = (unsigned)b;
+        for (int t = 0; t < tpb; t++) { threadIdx.x = t; kernel(); }
+    }
+}
+
+/* Parallel launch over blocks with OpenMP, for the grid update and G2P: their
+ * threads write disjoint data; the only shared writes are the disabled-point
+ * counter (atomic in the stub) and the error word, which these kernels touch
+ * only on NaN or out-of-cell errors. */
+template <class K> static void emulate_launch_parallel(size_t nthreads, int tpb, K kernel)
+{
+    const long long nblocks = (long long)((nthreads + tpb - 1) / tpb);
+#pragma omp parallel for schedule(static)
+    for (long long b = 0; b < nblocks; b++) {
+        blockDim.x = tpb;
         blockIdx.x = (unsigned)b;
         for (int t = 0; t < tpb; t++) { threadIdx.x = t; kernel(); }
     }
@@ -111,9 +132,9 @@ uint32_t ref_run_steps(const SimParams *prms, double *soa, size_t pitch, size_t 
         const float simulation_time = (float)(prms->InitialTimeStep * step);
         std::memset(grid, 0, gpitch * 3 * sizeof(double));
         emulate_launch(n, prms->tpb_P2G, [] { partition_kernel_p2g(); });
-        emulate_launch(nNodes, prms->tpb_Upd, [&] { partition_kernel_update_nodes(simulation_time); });
+        emulate_launch_parallel(nNodes, prms->tpb_Upd, [&] { partition_kernel_update_nodes(simulation_time); });
         const bool isCycleStart = step % prms->UpdateEveryNthStep == 0;
-        emulate_launch(n, prms->tpb_G2P, [&] { partition_kernel_g2p(isCycleStart); });
+        emulate_launch_parallel(n, prms->tpb_G2P, [&] { partition_kernel_g2p(isCycleStart); });
     }
     if (disabled) *disabled += gpu_disabled_points_count;
     return gpu_error_indicator;
@@ -130,6 +151,15 @@ unsigned ref_remove_disabled_and_sort(double *soa, unsigned capacity, unsigned s
     unsigned r = h.size;
     h.host_buffer = nullptr;  /* the buffer stays the caller's */
     return r;
+}
+
+int ref_num_threads(void)
+{
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
 }
 
 }  /* extern "C" */

@@ -60,6 +60,9 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=4)
+    ap.add_argument("--grid", type=int, nargs=2, default=None, metavar=("GX", "GY"),
+                    help="same scene rules on a smaller GX x GY grid (seeds scaled by area), "
+                         "for profiling captures")
     return ap.parse_args()
 
 
@@ -122,10 +125,13 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows), "power_w_max": max(pw) if pw else None}
 
 
-def make_scene(seed, max_points=None, sample=False):
+def make_scene(seed, max_points=None, sample=False, grid=None):
     from icempm_2d_sp_b200 import scenes
     if sample:  # the same generation rules on a 1024x512 sub-domain (1/16 of the cells)
         return scenes.config1(seed=seed, gx=1024, gy=512, n_seeds=125)
+    if grid is not None:
+        gx, gy = grid
+        return scenes.config1(seed=seed, gx=gx, gy=gy, n_seeds=max(1, round(2000 * gx * gy / (4096 * 2048))))
     return scenes.config1(seed=seed, max_points=max_points)
 
 
@@ -210,7 +216,7 @@ def main():
         if dist:
             dist.barrier()
 
-    sc = make_scene(1235 + rank, max_points=args.max_points)
+    sc = make_scene(1235 + rank, max_points=args.max_points, grid=args.grid)
     n, G = sc.n, sc.grid_nodes
     peak, peak_src = load_peaks()
 
@@ -283,11 +289,12 @@ def main():
         cpu = cpu_baseline(args, sc)
 
     if rank == 0:
+        workload = WORKLOAD if args.grid is None else WORKLOAD.replace("4096x2048", "%dx%d" % tuple(args.grid))
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic (seeded scene generator, BASELINE config 1 rules)",
-                "config": {"workload": WORKLOAD, "points": int(n), "points_all_ranks": n_tot, "grid_nodes": G,
+                "config": {"workload": workload, "points": int(n), "points_all_ranks": n_tot, "grid_nodes": G,
                            "variant": "fixed: int64 fixed-point P2G, FP32 state (chosen form)",
                            "forcing": "extended (Rankine wind, quadratic water drag)",
                            "parallelism": f"{world} independent scene(s), one per GPU",

@@ -14,12 +14,14 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
-BUILD = os.path.join(HERE, "_build")
-LIB = os.path.join(HERE, "libicempm_b200.so")
+BUILD = os.environ.get("ICEMPM_BUILD_DIR", os.path.join(HERE, "_build"))
+LIB = os.environ.get("ICEMPM_LIB_OUT", os.path.join(HERE, "libicempm_b200.so"))
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fvisibility=hidden",
          "--expt-relaxed-constexpr", "-I", os.path.join(ROOT, "include")]
+# developer knob for tuning builds, e.g. ICEMPM_EXTRA_FLAGS="-DICEMPM_FUSED_MINB=3"
+FLAGS += os.environ.get("ICEMPM_EXTRA_FLAGS", "").split()
 SOURCES = ["capi.cu", "engine_fixed.cu", "engine_fp32.cu", "engine_fp64.cu"]
 
 

@@ -11,7 +11,7 @@ import numpy as np
 from .params import SimParams, Options, N_PTS_ARRAYS
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libicempm_b200.so")
+LIB_PATH = os.environ.get("ICEMPM_LIBRARY", os.path.join(HERE, "libicempm_b200.so"))
 
 EXPORTS = [
     "icempm_default_options", "icempm_create", "icempm_destroy", "icempm_upload_points",

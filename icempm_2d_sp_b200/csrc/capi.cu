@@ -49,7 +49,7 @@ void icempm_default_options(icempm_options_t *o)
     o->forcing = ICEMPM_FORCING_COMPAT;
     o->sort_every = 0;
     o->use_graphs = 1;
-    o->block_threads = 256;
+    o->block_threads = 128;
     o->warp_reduce = 1;
     o->device = 0;
     o->water_density = 1025.0;
@@ -67,8 +67,8 @@ int icempm_create(const icempm_simparams_t *prms, const uint8_t *grid_status, co
     if (!prms || !grid_status) return fail(ICEMPM_E_ARG, "prms and grid_status are required");
     icempm_options_t o;
     if (opts) o = *opts; else icempm_default_options(&o);
-    if (o.block_threads != 0 && o.block_threads != 256)
-        return fail(ICEMPM_E_UNSUPPORTED, "block_threads must be 0 or 256");
+    if (o.block_threads != 0 && o.block_threads != 128)
+        return fail(ICEMPM_E_UNSUPPORTED, "block_threads must be 0 or 128");
     if (o.forcing != ICEMPM_FORCING_COMPAT && o.forcing != ICEMPM_FORCING_EXTENDED)
         return fail(ICEMPM_E_ARG, "unknown forcing");
     icempm::Engine *e = nullptr;

@@ -9,7 +9,7 @@
 #include <vector>
 #include <algorithm>
 
-#include "engine.cuh"
+#include "transfer.cuh"
 #include "engine_iface.h"
 
 namespace icempm {
@@ -24,8 +24,10 @@ static inline double pow2_floor(double x) { return std::ldexp(1.0, (int)std::flo
 
 template <class Real, class Acc>
 class EngineT final : public Engine {
-    static constexpr int BT = 256;       // points per CTA in the particle kernels
-    static constexpr int CAP = 512;      // nodes in the shared scatter tile
+    static constexpr int BT = 128;       // threads per CTA of the fused kernel
+    static constexpr int PPT = 4;        // points per thread of the fused kernel
+    static constexpr int CAP = 1024;     // nodes in the shared scatter tile
+    static constexpr int BT_P2G = 256;   // threads per CTA of the priming scatter
     static constexpr int GRAPH_STEPS = 32;
 
 public:
@@ -93,8 +95,9 @@ public:
                                                     (uint32_t *)nullptr, (uint32_t *)nullptr, (int)nc, 0, 64, stream_));
         sort_tmp_bytes_ = std::max(t32, t64);
         ICEMPM_CUDA(cudaMalloc(&sort_tmp_, sort_tmp_bytes_));
-        tile_.tx = 8; tile_.ty = 8;
-        if (opts_.block_threads == 128) { tile_.tx = 8; tile_.ty = 4; }
+        // a CTA of the fused kernel handles BT*PPT points, ~BT*PPT/4 cells at
+        // 4 points per cell: 8 columns of 16 cells
+        tile_.tx = 8; tile_.ty = BT * PPT / 32;
         tile_.ntiles_y = (gy_ + tile_.ty - 1) / tile_.ty;
         return set_params(p, 1.0);
     }
@@ -106,7 +109,7 @@ public:
         KParams<Real> &k = kp_;
         k.gx = gx_; k.gy = gy_;
         k.update_every = p.UpdateEveryNthStep;
-        k.forcing = opts_.forcing; k.wind_kind = opts_.wind_kind;
+        k.ext = opts_.forcing == ICEMPM_FORCING_EXTENDED; k.wind_kind = opts_.wind_kind;
         k.h = Real(p.cellsize); k.h_inv = Real(p.cellsize_inv);
         k.dt = Real(p.InitialTimeStep);
         k.dt_h_inv = Real(p.InitialTimeStep * p.cellsize_inv);
@@ -114,22 +117,22 @@ public:
         k.vmax2_01 = Real(p.vmax * p.vmax * 0.1);
         k.particle_mass = Real(p.ParticleMass);
         k.dt_vol_Dpinv = Real(p.dt_vol_Dpinv);
-        k.particle_volume = Real(p.ParticleVolume);
         k.dt_d = p.InitialTimeStep;
         k.kL = p.waterDragEffectiveLinear * p.InitialTimeStep;
         k.kQ = p.waterDragEffectiveQuadratic * p.InitialTimeStep;
         const double mref = std::max(p.ParticleMass * max_thick_, 1e-30);
         k.scale_m = pow2_floor(std::ldexp(1.0, 62) / (4096.0 * mref));
         k.scale_p = k.scale_m / 16.0;
-        k.scale_a = pow2_floor(std::ldexp(1.0, 62) / (4096.0 * std::max(p.ParticleVolume, 1e-30)));
-        k.inv_scale_m = 1.0 / k.scale_m; k.inv_scale_p = 1.0 / k.scale_p; k.inv_scale_a = 1.0 / k.scale_a;
-        k.lim_m = std::ldexp(1.0, 52) / k.scale_m;
-        k.lim_p = std::ldexp(1.0, 52) / k.scale_p;
-        k.rho_w_cd_dt = opts_.water_density * opts_.water_drag_coeff * p.InitialTimeStep;
-        k.rho_a_ca_dt = opts_.air_density * opts_.air_drag_coeff * p.InitialTimeStep;
-        k.wind_u = opts_.wind_u; k.wind_v = opts_.wind_v;
-        k.wind_cx = opts_.wind_cx; k.wind_cy = opts_.wind_cy;
-        k.wind_vmax = opts_.wind_vmax; k.wind_radius = opts_.wind_radius;
+        k.inv_scale_m = 1.0 / k.scale_m; k.inv_scale_p = 1.0 / k.scale_p;
+        // one term may use 2^56 of the 2^63 range: 64 worst-case terms fit a node
+        k.lim_m = (float)(std::ldexp(1.0, 56) / k.scale_m);
+        k.lim_p = (float)(std::ldexp(1.0, 56) / k.scale_p);
+        k.ext_impulse = Real(p.InitialTimeStep * p.ParticleVolume);
+        k.rho_w_cd = Real(opts_.water_density * opts_.water_drag_coeff);
+        k.rho_a_ca = Real(opts_.air_density * opts_.air_drag_coeff);
+        k.wind_u = Real(opts_.wind_u); k.wind_v = Real(opts_.wind_v);
+        k.wind_cx = Real(opts_.wind_cx); k.wind_cy = Real(opts_.wind_cy);
+        k.wind_vmax = Real(opts_.wind_vmax); k.wind_radius = Real(opts_.wind_radius);
         Material &m = k.mat;
         m.mu = p.mu; m.kappa = p.kappa; m.DP_threshold_p = p.DP_threshold_p;
         m.pmax = p.IceCompressiveStrength; m.pmin = -p.IceTensileStrength;
@@ -227,32 +230,20 @@ public:
         launches_++;
     }
 
-    template <int NCH, bool WR> void launch_fused_t()
-    {
-        const unsigned nb = (n_ + BT - 1) / BT;
-        k_g2p_p2g<Real, Acc, NCH, BT, CAP, WR><<<nb, BT, 0, stream_>>>(kp_, pts_[par_], grid(), st_, (int)n_);
-    }
     void launch_fused()
     {
-        const bool ext = opts_.forcing == ICEMPM_FORCING_EXTENDED;
-        const bool wr = opts_.warp_reduce != 0;
-        if (ext) { if (wr) launch_fused_t<4, true>(); else launch_fused_t<4, false>(); }
-        else { if (wr) launch_fused_t<3, true>(); else launch_fused_t<3, false>(); }
+        const size_t warps = ((size_t)n_ + 32 * PPT - 1) / (32 * PPT);
+        const unsigned nb = (unsigned)((warps + BT / 32 - 1) / (BT / 32));
+        k_g2p_p2g<Real, Acc, BT, PPT, CAP><<<nb, BT, 0, stream_>>>(kp_, pts_[par_], grid(), st_, (int)n_);
         launches_++;
-    }
-    template <int NCH, bool WR> void launch_p2g_t()
-    {
-        const unsigned nb = (n_ + BT - 1) / BT;
-        k_p2g<Real, Acc, NCH, BT, CAP, WR><<<nb, BT, 0, stream_>>>(kp_, pts_[par_], grid(), st_, (int)n_);
     }
     int prime()
     {
         ICEMPM_CUDA(cudaMemsetAsync(acc_, 0, G_ * sizeof(Acc4<Acc>), stream_));
+        ICEMPM_CUDA(cudaMemsetAsync(&st_->err_pending, 0, sizeof(uint32_t), stream_));
         if (n_ > 0) {
-            const bool ext = opts_.forcing == ICEMPM_FORCING_EXTENDED;
-            const bool wr = opts_.warp_reduce != 0;
-            if (ext) { if (wr) launch_p2g_t<4, true>(); else launch_p2g_t<4, false>(); }
-            else { if (wr) launch_p2g_t<3, true>(); else launch_p2g_t<3, false>(); }
+            const unsigned nb = (n_ + BT_P2G - 1) / BT_P2G;
+            k_p2g<Real, Acc, BT_P2G, CAP><<<nb, BT_P2G, 0, stream_>>>(kp_, pts_[par_], grid(), st_, (int)n_);
             launches_++;
             ICEMPM_CUDA(cudaGetLastError());
         }
@@ -408,7 +399,8 @@ public:
         return 0;
     }
 
-    // Sort by the tiled locality key into the other parity (host slots unchanged).
+    // Sort by the tiled locality key into the other parity, in the fused
+    // kernel's interleaved order (host slots unchanged).
     int locality_sort()
     {
         if (n_ == 0) return 0;
@@ -419,7 +411,7 @@ public:
         size_t tb = sort_tmp_bytes_;
         ICEMPM_CUDA(cub::DeviceRadixSort::SortPairs(sort_tmp_, tb, k32in, k32out, vals_[0], vals_[1], (int)n_, 0, 32, stream_));
         launches_ += 4;
-        k_gather<Real><<<nb, 256, 0, stream_>>>(pts_[par_], pts_[1 - par_], vals_[1], (int)n_, 0);
+        k_gather<Real><<<nb, 256, 0, stream_>>>(pts_[par_], pts_[1 - par_], vals_[1], (int)n_, 0, PPT);
         launches_++;
         ICEMPM_CUDA(cudaGetLastError());
         par_ = 1 - par_;
@@ -438,7 +430,7 @@ public:
             size_t tb = sort_tmp_bytes_;
             ICEMPM_CUDA(cub::DeviceRadixSort::SortPairs(sort_tmp_, tb, keys_[0], keys_[1], vals_[0], vals_[1], (int)n_, 0, 64, stream_));
             launches_ += 4;
-            k_gather<Real><<<nb, 256, 0, stream_>>>(pts_[par_], pts_[1 - par_], vals_[1], (int)n_, 1);
+            k_gather<Real><<<nb, 256, 0, stream_>>>(pts_[par_], pts_[1 - par_], vals_[1], (int)n_, 1, 0);
             k_count_active<<<nb, 256, 0, stream_>>>(keys_[1], (int)n_, st_);
             launches_ += 2;
             ICEMPM_CUDA(cudaGetLastError());

@@ -319,8 +319,10 @@ int orc_wolper_dp(const SP *p, double thickness, double p_tr, double q_tr, doubl
 
 /* Scatter of one point; returns error bits.  area (may be NULL) receives
  * sum(w * ParticleVolume) for the extended forcing. */
+static void wind_at(const icempm_options_t *o, double x, double y, double *ux, double *uy);
+
 static uint32_t p2g_point(const SP *p, const double *soa, size_t pitch, size_t i,
-                          double *grid, size_t gpitch, size_t nnodes, double *area)
+                          double *grid, size_t gpitch, size_t nnodes, const icempm_options_t *ext)
 {
     uint32_t err = 0;
     const double h = p->cellsize;
@@ -347,6 +349,27 @@ static uint32_t p2g_point(const SP *p, const double *soa, size_t pitch, size_t i
     double sub[4];
     for (int k = 0; k < 4; k++) sub[k] = particle_mass * Bp[k] - sc * PFt[k];
 
+    /* extended forcing: impulse of the wind and water stresses over the
+       point's area during the step, distributed with the B-spline weights */
+    double fx = 0, fy = 0;
+    if (ext) {
+        double ux, uy;
+        wind_at(ext, (cx + pos[0]) * h, (cy + pos[1]) * h, &ux, &uy);
+        const double um = sqrt(ux * ux + uy * uy);
+        const long long nc = (long long)cy + (long long)cx * gridY;
+        double wx = 0, wy = 0;
+        if (nc >= 0 && (size_t)nc < nnodes) {
+            wx = grid[ICEMPM_GRID_CURRENT_VX * gpitch + nc];
+            wy = grid[ICEMPM_GRID_CURRENT_VY * gpitch + nc];
+        }
+        const double dx = wx - vel[0], dy = wy - vel[1];
+        const double dm = sqrt(dx * dx + dy * dy);
+        const double ca = ext->air_density * ext->air_drag_coeff * um;
+        const double cw = ext->water_density * ext->water_drag_coeff * dm;
+        const double f = p->InitialTimeStep * p->ParticleVolume;
+        fx = f * (ca * ux + cw * dx);
+        fy = f * (ca * uy + cw * dy);
+    }
     double ww[3][2];
     orc_weights(pos, ww);
     for (int a = -1; a <= 1; a++)
@@ -354,14 +377,14 @@ static uint32_t p2g_point(const SP *p, const double *soa, size_t pitch, size_t i
             const double Wip = ww[a + 1][0] * ww[b + 1][1];
             const double incM = Wip * particle_mass;
             const double d0 = (a - pos[0]) * h, d1 = (b - pos[1]) * h;
-            const double incV0 = Wip * (vel[0] * particle_mass + (sub[0] * d0 + sub[1] * d1));
-            const double incV1 = Wip * (vel[1] * particle_mass + (sub[2] * d0 + sub[3] * d1));
+            double incV0 = Wip * (vel[0] * particle_mass + (sub[0] * d0 + sub[1] * d1));
+            double incV1 = Wip * (vel[1] * particle_mass + (sub[2] * d0 + sub[3] * d1));
+            if (ext) { incV0 += Wip * fx; incV1 += Wip * fy; }
             const long long node = (long long)(b + cy) + (long long)(a + cx) * gridY;
             if (node >= 0 && (size_t)node < nnodes) {
                 grid[ICEMPM_GRID_MASS * gpitch + node] += incM;
                 grid[ICEMPM_GRID_PX * gpitch + node] += incV0;
                 grid[ICEMPM_GRID_PY * gpitch + node] += incV1;
-                if (area) area[node] += Wip * p->ParticleVolume;
             }
             if (isnan(incV0) || isnan(incV1)) err |= ICEMPM_ERR_GRID_P2G_NAN_VEL;
             if (isnan(incM)) err |= ICEMPM_ERR_GRID_P2G_NAN_MASS;
@@ -374,7 +397,7 @@ static uint32_t p2g_point(const SP *p, const double *soa, size_t pitch, size_t i
 
 /* P2G over all enabled points.  Deterministic, see the file header. */
 uint32_t orc_p2g(const SP *p, const double *soa, size_t pitch, size_t n,
-                 double *grid, size_t gpitch, double *area)
+                 double *grid, size_t gpitch, const icempm_options_t *ext)
 {
     const int gx = p->GridXTotal;
     const size_t nnodes = (size_t)gx * p->GridYTotal;
@@ -406,7 +429,7 @@ uint32_t orc_p2g(const SP *p, const double *soa, size_t pitch, size_t n,
 #pragma omp parallel for schedule(dynamic, 1) reduction(| : e)
         for (int s = color; s < nstrips; s += 2)
             for (size_t k = start[s]; k < start[s + 1]; k++)
-                e |= p2g_point(p, soa, pitch, order[k], grid, gpitch, nnodes, area);
+                e |= p2g_point(p, soa, pitch, order[k], grid, gpitch, nnodes, ext);
         err |= e;
     }
     free(start); free(sid); free(order);
@@ -472,20 +495,15 @@ static void wind_at(const icempm_options_t *o, double x, double y, double *ux, d
     }
 }
 
-/* Extended grid update (no reference counterpart; the reference computes a
- * wind vector but never passes it to the kernel, gpu_partition.cpp:336-348):
- *   v   = p/m
- *   v  += dt * rho_a Ca |Ua| Ua * A/m                  (wind stress, explicit)
- *   dU  = v_w - v ;  k = dt * rho_w Cd |dU| * A/m
- *   v  += k/(1+k) * dU                                 (water drag, linearly implicit)
- * with A = sum_p w_ip * ParticleVolume the ice area carried by the node.
- * Walls and the velocity clamp are as in the compat update. */
-uint32_t orc_update_nodes_ext(const SP *p, const icempm_options_t *o, double *grid, size_t gpitch,
-                              const uint8_t *status, const double *area)
+/* Grid update of the extended forcing (no reference counterpart; the
+ * reference computes a wind vector but never passes it to the kernel,
+ * gpu_partition.cpp:336-348).  The wind and water stresses enter as point
+ * impulses in P2G (p2g_point), so the node update is v = p/m with the
+ * reference's walls and velocity clamp and neither the current ramp nor the
+ * effective-coefficient drag. */
+uint32_t orc_update_nodes_ext(const SP *p, double *grid, size_t gpitch, const uint8_t *status)
 {
-    const int gy = p->GridYTotal;
-    const long long nNodes = (long long)p->GridXTotal * gy;
-    const double dt = p->InitialTimeStep, h = p->cellsize;
+    const long long nNodes = (long long)p->GridXTotal * p->GridYTotal;
     uint32_t err = 0;
 #pragma omp parallel for schedule(static) reduction(| : err)
     for (long long idx = 0; idx < nNodes; idx++) {
@@ -498,18 +516,6 @@ uint32_t orc_update_nodes_ext(const SP *p, const icempm_options_t *o, double *gr
             v0 = 0; v1 = 0;
             grid[ICEMPM_GRID_FX * gpitch + idx] += mx;
             grid[ICEMPM_GRID_FY * gpitch + idx] += my;
-        } else {
-            const double am = area[idx] / mass;
-            double ux, uy;
-            wind_at(o, (double)(idx / gy) * h, (double)(idx % gy) * h, &ux, &uy);
-            const double um = sqrt(ux * ux + uy * uy);
-            const double ta = dt * o->air_density * o->air_drag_coeff * um * am;
-            v0 += ta * ux; v1 += ta * uy;
-            const double d0 = grid[ICEMPM_GRID_CURRENT_VX * gpitch + idx] - v0;
-            const double d1 = grid[ICEMPM_GRID_CURRENT_VY * gpitch + idx] - v1;
-            const double k = dt * o->water_density * o->water_drag_coeff * sqrt(d0 * d0 + d1 * d1) * am;
-            const double f = k / (1 + k);
-            v0 += f * d0; v1 += f * d1;
         }
         if (v0 * v0 + v1 * v1 > p->vmax * p->vmax * 0.1) { v0 = 0; v1 = 0; }
         grid[ICEMPM_GRID_PX * gpitch + idx] = v0;
@@ -638,20 +644,18 @@ uint32_t orc_run_steps(const SP *p, const icempm_options_t *opts, double *soa, s
 {
     uint32_t err = 0;
     const size_t nn = (size_t)p->GridXTotal * p->GridYTotal;
-    const int ext = opts && opts->forcing == ICEMPM_FORCING_EXTENDED;
-    double *area = ext ? (double *)malloc(nn * sizeof(double)) : NULL;
+    const icempm_options_t *ext = (opts && opts->forcing == ICEMPM_FORCING_EXTENDED) ? opts : NULL;
+    (void)nn;
     for (int k = 0; k < nsteps; k++) {
         const int step = first_step + k;
         const double t = (double)(float)(p->InitialTimeStep * step);
         memset(grid, 0, 3 * gpitch * sizeof(double)); /* mass, px, py (gpu_partition.cpp:300-308) */
-        if (area) memset(area, 0, nn * sizeof(double));
-        err |= orc_p2g(p, soa, pitch, n, grid, gpitch, area);
-        if (ext) err |= orc_update_nodes_ext(p, opts, grid, gpitch, status, area);
+        err |= orc_p2g(p, soa, pitch, n, grid, gpitch, ext);
+        if (ext) err |= orc_update_nodes_ext(p, grid, gpitch, status);
         else err |= orc_update_nodes(p, grid, gpitch, status, t);
         const int recordPQ = (p->UpdateEveryNthStep > 0) ? (step % p->UpdateEveryNthStep == 0) : 0;
         err |= orc_g2p(p, soa, pitch, n, grid, gpitch, recordPQ, disabled_count);
     }
-    free(area);
     return err;
 }
 

@@ -39,11 +39,11 @@ def lib():
         L.orc_wolper_dp.argtypes = [sp, C.c_double, C.c_double, C.c_double, C.c_double,
                                     dp, dp, dp, dp, dp, dp, C.POINTER(C.c_int)]
         L.orc_wolper_dp.restype = C.c_int
-        L.orc_p2g.argtypes = [sp, dp, C.c_size_t, C.c_size_t, dp, C.c_size_t, dp]
+        L.orc_p2g.argtypes = [sp, dp, C.c_size_t, C.c_size_t, dp, C.c_size_t, C.POINTER(Options)]
         L.orc_p2g.restype = C.c_uint32
         L.orc_update_nodes.argtypes = [sp, dp, C.c_size_t, u8p, C.c_double]
         L.orc_update_nodes.restype = C.c_uint32
-        L.orc_update_nodes_ext.argtypes = [sp, C.POINTER(Options), dp, C.c_size_t, u8p, dp]
+        L.orc_update_nodes_ext.argtypes = [sp, dp, C.c_size_t, u8p]
         L.orc_update_nodes_ext.restype = C.c_uint32
         L.orc_g2p.argtypes = [sp, dp, C.c_size_t, C.c_size_t, dp, C.c_size_t, C.c_int,
                               C.POINTER(C.c_int32)]
@@ -138,18 +138,18 @@ def new_grid(p: SimParams, status=None, current=None):
     return grid
 
 
-def p2g(p, soa, n, grid, area=None):
-    ap = _dp(area) if area is not None else None
-    return lib().orc_p2g(C.byref(p), _dp(soa), soa.shape[1], n, _dp(grid), grid.shape[1], ap)
+def p2g(p, soa, n, grid, opts=None):
+    """P2G into grid rows 0-2; opts with extended forcing adds the stress impulses."""
+    ext = C.byref(opts) if (opts is not None and opts.forcing == 1) else None
+    return lib().orc_p2g(C.byref(p), _dp(soa), soa.shape[1], n, _dp(grid), grid.shape[1], ext)
 
 
 def update_nodes(p, grid, status, t):
     return lib().orc_update_nodes(C.byref(p), _dp(grid), grid.shape[1], _u8p(status), float(t))
 
 
-def update_nodes_ext(p, opts, grid, status, area):
-    return lib().orc_update_nodes_ext(C.byref(p), C.byref(opts), _dp(grid), grid.shape[1],
-                                      _u8p(status), _dp(area))
+def update_nodes_ext(p, grid, status):
+    return lib().orc_update_nodes_ext(C.byref(p), _dp(grid), grid.shape[1], _u8p(status))
 
 
 def g2p(p, soa, n, grid, recordPQ):

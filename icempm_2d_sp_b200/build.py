@@ -23,6 +23,9 @@ FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fvisibility=hid
 # developer knob for tuning builds, e.g. ICEMPM_EXTRA_FLAGS="-DICEMPM_FUSED_MINB=3"
 FLAGS += os.environ.get("ICEMPM_EXTRA_FLAGS", "").split()
 SOURCES = ["capi.cu", "engine_fixed.cu", "engine_fp32.cu", "engine_fp64.cu"]
+# The FP32-state engines use approximate single-precision division and square
+# root (a few ulp, far inside the parity tolerances); the FP64 engine is exact.
+PER_SOURCE = {"engine_fixed.cu": ["-use_fast_math"], "engine_fp32.cu": ["-use_fast_math"]}
 
 
 def _deps():
@@ -34,7 +37,7 @@ def _deps():
 
 def _compile(src: str, verbose: bool) -> str:
     obj = os.path.join(BUILD, os.path.splitext(src)[0] + ".o")
-    cmd = [NVCC] + ARCH + FLAGS + ["-c", os.path.join(CSRC, src), "-o", obj]
+    cmd = [NVCC] + ARCH + FLAGS + PER_SOURCE.get(src, []) + ["-c", os.path.join(CSRC, src), "-o", obj]
     if verbose:
         cmd += ["-Xptxas", "-v"]
     r = subprocess.run(cmd, capture_output=True, text=True)

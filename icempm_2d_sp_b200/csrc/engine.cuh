@@ -37,9 +37,13 @@
 #include "device_math.cuh"
 #include "../../include/icempm.h"
 
-// CTAs per SM the fused kernel is compiled for (FP32 state; FP64 keeps 1).
+// CTAs per SM the fused kernel is compiled for (FP32 state; FP64 keeps 1),
+// and points per thread of the fused kernel.
 #ifndef ICEMPM_FUSED_MINB
-#define ICEMPM_FUSED_MINB 6
+#define ICEMPM_FUSED_MINB 5
+#endif
+#ifndef ICEMPM_FUSED_PPT
+#define ICEMPM_FUSED_PPT 8
 #endif
 
 namespace icempm {
@@ -47,6 +51,42 @@ namespace icempm {
 template <class T> struct alignas(16) V4 { T x, y, z, w; };
 template <class T> struct alignas(2 * sizeof(T) > 16 ? 16 : 2 * sizeof(T)) V2 { T x, y; };
 template <class A> struct alignas(16) Acc4 { A m, px, py, pad; };
+
+// Point arrays are read once and written once per step: load and store them
+// with the streaming cache policy so they do not evict the grid velocities
+// the 3x3 gathers reuse from L1.
+__device__ __forceinline__ V4<float> ld_stream(const V4<float> *p)
+{
+    const float4 v = __ldcs(reinterpret_cast<const float4 *>(p));
+    V4<float> r; r.x = v.x; r.y = v.y; r.z = v.z; r.w = v.w;
+    return r;
+}
+__device__ __forceinline__ V4<double> ld_stream(const V4<double> *p)
+{
+    const double2 a = __ldcs(reinterpret_cast<const double2 *>(p));
+    const double2 b = __ldcs(reinterpret_cast<const double2 *>(p) + 1);
+    V4<double> r; r.x = a.x; r.y = a.y; r.z = b.x; r.w = b.y;
+    return r;
+}
+__device__ __forceinline__ uint2 ld_stream(const uint2 *p) { return __ldcs(p); }
+__device__ __forceinline__ void st_stream(V4<float> *p, const V4<float> &v)
+{
+    __stcs(reinterpret_cast<float4 *>(p), make_float4(v.x, v.y, v.z, v.w));
+}
+__device__ __forceinline__ void st_stream(V4<double> *p, const V4<double> &v)
+{
+    __stcs(reinterpret_cast<double2 *>(p), make_double2(v.x, v.y));
+    __stcs(reinterpret_cast<double2 *>(p) + 1, make_double2(v.z, v.w));
+}
+__device__ __forceinline__ void st_stream(V2<float> *p, const V2<float> &v)
+{
+    __stcs(reinterpret_cast<float2 *>(p), make_float2(v.x, v.y));
+}
+__device__ __forceinline__ void st_stream(V2<double> *p, const V2<double> &v)
+{
+    __stcs(reinterpret_cast<double2 *>(p), make_double2(v.x, v.y));
+}
+__device__ __forceinline__ void st_stream(uint2 *p, const uint2 &v) { __stcs(p, v); }
 
 struct DevStatus {
     uint32_t err;          // the reference's gpu_error_indicator
@@ -70,6 +110,7 @@ template <class Real, class Acc> struct Grid {
     Acc4<Acc> *acc;
     V2<Real> *vel;
     V2<Real> *cur;
+    const V4<Real> *frc;   // extended forcing per node: {current vx, vy, wind stress x, y}
     const uint8_t *status;
     double2 *force;
 };
@@ -85,8 +126,7 @@ template <class Real> struct KParams {
     double inv_scale_m, inv_scale_p;
     float lim_m, lim_p;             // largest |value| a single term may carry in fixed point
     Real ext_impulse;               // dt * ParticleVolume (extended forcing)
-    Real rho_a_ca, rho_w_cd;        // extended forcing coefficients
-    Real wind_u, wind_v, wind_cx, wind_cy, wind_vmax, wind_radius;
+    Real rho_w_cd;                  // rho_w * Cd (extended forcing)
     Material mat;
 };
 
@@ -139,29 +179,14 @@ __device__ __forceinline__ bool cell_in_range(int cx, int cy, int gx, int gy)
     return cx >= 1 && cx <= gx - 2 && cy >= 1 && cy <= gy - 2;
 }
 
-template <class Real>
-__device__ __forceinline__ void wind_at(const KParams<Real> &kp, Real x, Real y, Real &ux, Real &uy)
-{
-    ux = Real(0); uy = Real(0);
-    if (kp.wind_kind == ICEMPM_WIND_UNIFORM) { ux = kp.wind_u; uy = kp.wind_v; }
-    else if (kp.wind_kind == ICEMPM_WIND_RANKINE) {
-        const Real dx = x - kp.wind_cx, dy = y - kp.wind_cy;
-        const Real r = tsqrt(dx * dx + dy * dy);
-        if (r > Real(0)) {
-            const Real sp = (r < kp.wind_radius) ? kp.wind_vmax * r / kp.wind_radius
-                                                 : kp.wind_vmax * kp.wind_radius / r;
-            ux = -dy / r * sp; uy = dx / r * sp;
-        }
-    }
-}
-
 // ---- P2G sources of one point --------------------------------------------
 // The reference scatters, for node offsets (i, j) in {-1,0,1}^2 (kernels.cuh:76-95)
 //   dM = w m_p,   dP = w (m_p v + S (i - x, j - y) h),
 //   S = m_p C - dt_vol_Dpinv Jp_inv thickness tau.
 // With A = m_p v - h S (x, y):  dP = w (A + h S (i, j)).  The extended
-// forcing adds the impulse dt * area * (wind + water stress) to A.  For
-// fixed-point accumulation the sources carry the accumulator scale already.
+// forcing adds the impulse dt * area * (wind + water stress) to A, with the
+// wind stress and the current of the point's cell node.  For fixed-point
+// accumulation the sources carry the accumulator scale already.
 template <class Real> struct Src {
     int cx, cy;
     Real wx[3], wy[3];
@@ -169,7 +194,7 @@ template <class Real> struct Src {
 };
 
 template <class Real, class Acc>
-__device__ __forceinline__ void make_src(const KParams<Real> &kp, const V2<Real> *__restrict__ cur, Src<Real> &s,
+__device__ __forceinline__ void make_src(const KParams<Real> &kp, const V4<Real> *__restrict__ frc, Src<Real> &s,
                                          Real x, Real y, Real Jp, Real thick, const Kin<Real> &k, Real vx,
                                          Real vy, Real c00, Real c01, Real c10, Real c11, uint32_t &perr)
 {
@@ -181,14 +206,11 @@ __device__ __forceinline__ void make_src(const KParams<Real> &kp, const V2<Real>
     Real ax = mp * vx - kp.h * (S00 * x + S01 * y);
     Real ay = mp * vy - kp.h * (S10 * x + S11 * y);
     if (kp.ext) {
-        Real ux, uy;
-        wind_at(kp, (Real(s.cx) + x) * kp.h, (Real(s.cy) + y) * kp.h, ux, uy);
-        const V2<Real> c = cur[(size_t)s.cx * kp.gy + s.cy];
-        const Real dx = c.x - vx, dy = c.y - vy;
-        const Real ca = kp.rho_a_ca * tsqrt(ux * ux + uy * uy);
+        const V4<Real> f = frc[(uint32_t)s.cx * (uint32_t)kp.gy + (uint32_t)s.cy];
+        const Real dx = f.x - vx, dy = f.y - vy;
         const Real cw = kp.rho_w_cd * tsqrt(dx * dx + dy * dy);
-        ax += kp.ext_impulse * (ca * ux + cw * dx);
-        ay += kp.ext_impulse * (ca * uy + cw * dy);
+        ax += kp.ext_impulse * (f.z + cw * dx);
+        ay += kp.ext_impulse * (f.w + cw * dy);
     }
     const Real fm = AccOps<Acc>::fixed ? Real(kp.scale_m) : Real(1);
     const Real fp = AccOps<Acc>::fixed ? Real(kp.scale_p) : Real(1);
@@ -236,7 +258,7 @@ __device__ __forceinline__ void node_add(const Tile<Acc, CAP> &T, bool in_tile, 
         AccOps<Acc>::add_shared(&T.t[1][li], ax);
         AccOps<Acc>::add_shared(&T.t[2][li], ay);
     } else {
-        const size_t node = (size_t)X * gy + (size_t)Y;
+        const uint32_t node = (uint32_t)X * (uint32_t)gy + (uint32_t)Y;
         AccOps<Acc>::add_global(&gacc[node].m, am);
         AccOps<Acc>::add_global(&gacc[node].px, ax);
         AccOps<Acc>::add_global(&gacc[node].py, ay);
@@ -263,7 +285,7 @@ __device__ __forceinline__ void tile_flush(const Tile<Acc, CAP> &T, Acc4<Acc> *_
         const int X = T.x0 + lx, Y = T.y0 + ly;
         const Acc m = T.t[0][k], px = T.t[1][k], py = T.t[2][k];
         if ((m != Acc(0) || px != Acc(0) || py != Acc(0)) && X >= 0 && X < gx && Y >= 0 && Y < gy) {
-            const size_t node = (size_t)X * gy + (size_t)Y;
+            const uint32_t node = (uint32_t)X * (uint32_t)gy + (uint32_t)Y;
             if (m != Acc(0)) AccOps<Acc>::add_global(&gacc[node].m, m);
             if (px != Acc(0)) AccOps<Acc>::add_global(&gacc[node].px, px);
             if (py != Acc(0)) AccOps<Acc>::add_global(&gacc[node].py, py);
@@ -330,7 +352,7 @@ __global__ void __launch_bounds__(BT) k_p2g(KParams<Real> kp, Pts<Real> P, Grid<
                 const V4<Real> A = P.A[i], Hv = P.H[i], Cv = P.C[i];
                 const V2<Real> v = P.V[i];
                 const M2<Real> H = {Hv.x, Hv.y, Hv.z, Hv.w};
-                make_src<Real, Acc>(kp, G.cur, s, A.x, A.y, A.z, A.w, kinematics(H), v.x, v.y,
+                make_src<Real, Acc>(kp, G.frc, s, A.x, A.y, A.z, A.w, kinematics(H), v.x, v.y,
                                     Cv.x, Cv.y, Cv.z, Cv.w, perr);
                 active = true;
             } else {
@@ -425,9 +447,9 @@ __global__ void __launch_bounds__(256) k_grid_update(KParams<Real> kp, Grid<Real
 // thread's PPT points are consecutive in the tiled cell order (mostly one
 // or two cells of one column) while every load and store of a warp stays
 // one contiguous 32-element access.
-template <int PPT> __host__ __device__ __forceinline__ size_t fused_index(size_t warp, int lane, int j)
+template <int PPT> __host__ __device__ __forceinline__ uint32_t fused_index(uint32_t warp, int lane, int j)
 {
-    return warp * (size_t)(32 * PPT) + (size_t)j * 32 + (size_t)lane;
+    return warp * (uint32_t)(32 * PPT) + (uint32_t)(j * 32 + lane);
 }
 
 // A thread accumulates its points' node terms in a register patch of the
@@ -506,7 +528,7 @@ k_g2p_p2g(KParams<Real> kp, Pts<Real> P, Grid<Real, Acc> G, DevStatus *st, int n
     __shared__ int box[4];
     init_box(box);
     const int lane = threadIdx.x & 31;
-    const size_t warp = ((size_t)blockIdx.x * BT + threadIdx.x) >> 5;
+    const uint32_t warp = (blockIdx.x * BT + threadIdx.x) >> 5;
 
     // tile from the current cells: a point moves at most one cell per step,
     // so its new 3x3 stencil lies within its old cell +- 2 nodes
@@ -514,8 +536,8 @@ k_g2p_p2g(KParams<Real> kp, Pts<Real> P, Grid<Real, Acc> G, DevStatus *st, int n
     bool any = false;
 #pragma unroll
     for (int j = 0; j < PPT; j++) {
-        const size_t i = fused_index<PPT>(warp, lane, j);
-        if (i < (size_t)n) {
+        const uint32_t i = fused_index<PPT>(warp, lane, j);
+        if (i < (uint32_t)n) {
             const uint2 key = P.K[i];
             const int cx = (int)(key.x & 0xffff), cy = (int)(key.x >> 16);
             if (!(key.y & kDisabled) && cell_in_range(cx, cy, kp.gx, kp.gy)) {
@@ -537,15 +559,24 @@ k_g2p_p2g(KParams<Real> kp, Pts<Real> P, Grid<Real, Acc> G, DevStatus *st, int n
     Patch<Real> patch;
     patch.have = false; patch.in_tile = false; patch.cx = patch.cy = 0;
 
+    // the next point's state is loaded one iteration ahead
+    uint32_t inext = fused_index<PPT>(warp, lane, 0);
+    bool vnext = inext < (uint32_t)n;
+    uint2 knext = make_uint2(0u, kDisabled);
+    V4<Real> anext, hnext;
+    if (vnext) { knext = ld_stream(P.K + inext); anext = ld_stream(P.A + inext); hnext = ld_stream(P.H + inext); }
 #pragma unroll 1
     for (int j = 0; j < PPT; j++) {
-        const size_t i = fused_index<PPT>(warp, lane, j);
-        if (i >= (size_t)n) break;
-        const uint2 key = P.K[i];
+        if (!vnext) break;
+        const uint32_t i = inext;
+        const uint2 key = knext;
+        const V4<Real> A = anext;
+        const V4<Real> Hv = hnext;
+        inext = fused_index<PPT>(warp, lane, j + 1);
+        vnext = j + 1 < PPT && inext < (uint32_t)n;
+        if (vnext) { knext = ld_stream(P.K + inext); anext = ld_stream(P.A + inext); hnext = ld_stream(P.H + inext); }
         uint32_t util = key.y;
         if (util & kDisabled) continue;
-        const V4<Real> A = P.A[i];
-        const V4<Real> Hv = P.H[i];
         Real x = A.x, y = A.y, Jp = A.z;
         const Real thick = A.w;
         M2<Real> H = {Hv.x, Hv.y, Hv.z, Hv.w};
@@ -558,7 +589,7 @@ k_g2p_p2g(KParams<Real> kp, Pts<Real> P, Grid<Real, Acc> G, DevStatus *st, int n
             V2<Real> nv[3][3];
 #pragma unroll
             for (int a = 0; a < 3; a++) {
-                const size_t col = (size_t)(cx + a - 1) * kp.gy + (size_t)(cy - 1);
+                const uint32_t col = (uint32_t)(cx + a - 1) * (uint32_t)kp.gy + (uint32_t)(cy - 1);
 #pragma unroll
                 for (int b = 0; b < 3; b++) nv[a][b] = G.vel[col + b];
             }
@@ -585,9 +616,9 @@ k_g2p_p2g(KParams<Real> kp, Pts<Real> P, Grid<Real, Acc> G, DevStatus *st, int n
         }
         x += vx * kp.dt_h_inv;
         y += vy * kp.dt_h_inv;
-        if (isnan(vx) || isnan(vy)) err |= kErrVelNan;
-        if (isnan(x) || isnan(y)) err |= kErrPosNan;
-        if (isnan(c00) || isnan(c10) || isnan(c01) || isnan(c11)) err |= kErrBpNan;
+        if (isnan(vx + vy)) err |= kErrVelNan;
+        if (isnan(x + y)) err |= kErrPosNan;
+        if (isnan((c00 + c10) + (c01 + c11))) err |= kErrBpNan;
         bool moved = false;
         if (x > Real(0.5)) { x -= Real(1); cx++; moved = true; }
         else if (x < Real(-0.5)) { x += Real(1); cx--; moved = true; }
@@ -608,7 +639,7 @@ k_g2p_p2g(KParams<Real> kp, Pts<Real> P, Grid<Real, Acc> G, DevStatus *st, int n
             H.a10 = h.a10 + d10 + (d10 * h.a00 + d11 * h.a10);
             H.a11 = h.a11 + d11 + (d10 * h.a01 + d11 * h.a11);
         }
-        if (isnan(H.a00) || isnan(H.a10) || isnan(H.a01) || isnan(H.a11)) err |= kErrFeNan;
+        if (isnan((H.a00 + H.a10) + (H.a01 + H.a11))) err |= kErrFeNan;
         Kin<Real> k = kinematics(H);
         Real p_tr, q_tr;
         pq(k, Real(kp.mat.mu), Real(kp.mat.kappa), p_tr, q_tr);
@@ -616,36 +647,34 @@ k_g2p_p2g(KParams<Real> kp, Pts<Real> P, Grid<Real, Acc> G, DevStatus *st, int n
         if (util & kCrushed) {
             const SvdH<Real> sv = svd_h(H);
             wolper_dp(kp.mat, thick, p_tr, q_tr, k, sv, H, Jp);
-            if (isnan(H.a00) || isnan(H.a10) || isnan(H.a01) || isnan(H.a11)) err |= kErrFeNan;
+            if (isnan((H.a00 + H.a10) + (H.a01 + H.a11))) err |= kErrFeNan;
             k = kinematics(H);
         }
 
         V4<Real> Ao; Ao.x = x; Ao.y = y; Ao.z = Jp; Ao.w = thick;
-        P.A[i] = Ao;
+        st_stream(P.A + i, Ao);
         V4<Real> Ho; Ho.x = H.a00; Ho.y = H.a01; Ho.z = H.a10; Ho.w = H.a11;
-        P.H[i] = Ho;
+        st_stream(P.H + i, Ho);
         V2<Real> Vo; Vo.x = vx; Vo.y = vy;
-        P.V[i] = Vo;
+        st_stream(P.V + i, Vo);
         V4<Real> Co; Co.x = c00; Co.y = c01; Co.z = c10; Co.w = c11;
-        P.C[i] = Co;
+        st_stream(P.C + i, Co);
         const uint32_t cell = ((uint32_t)cy << 16) | (uint32_t)cx;   // as kernels.cuh:305
         if (moved || util != key.y) {
             uint2 ko; ko.x = moved ? cell : key.x; ko.y = util;
-            P.K[i] = ko;
+            st_stream(P.K + i, ko);
         }
-        if (recordPQ) { V2<Real> pqv; pqv.x = p_tr; pqv.y = q_tr; P.PQ[i] = pqv; }
+        if (recordPQ) { V2<Real> pqv; pqv.x = p_tr; pqv.y = q_tr; st_stream(P.PQ + i, pqv); }
 
         if (!(util & kDisabled)) {
             if (cell_in_range(cx, cy, kp.gx, kp.gy)) {
                 Src<Real> s;
                 s.cx = cx; s.cy = cy;
-                make_src<Real, Acc>(kp, G.cur, s, x, y, Jp, thick, k, vx, vy, c00, c01, c10, c11, perr);
-                const bool nan_w = isnan(s.wx[0]) || isnan(s.wx[1]) || isnan(s.wx[2]) ||
-                                   isnan(s.wy[0]) || isnan(s.wy[1]) || isnan(s.wy[2]);
-                if (nan_w || isnan(s.mp)) perr |= kErrP2gNanMass;
-                if (nan_w || isnan(s.ax) || isnan(s.ay) || isnan(s.s00) || isnan(s.s01) || isnan(s.s10) ||
-                    isnan(s.s11))
-                    perr |= kErrP2gNanVel;
+                make_src<Real, Acc>(kp, G.frc, s, x, y, Jp, thick, k, vx, vy, c00, c01, c10, c11, perr);
+                // NaN reaches these sums from any NaN term (the scatter's NaN checks)
+                const Real sw = (s.wx[0] + s.wx[1] + s.wx[2]) + (s.wy[0] + s.wy[1] + s.wy[2]);
+                if (isnan(sw + s.mp)) perr |= kErrP2gNanMass;
+                if (isnan(sw + ((s.ax + s.ay) + (s.s00 + s.s01) + (s.s10 + s.s11)))) perr |= kErrP2gNanVel;
                 patch_add<Real, Acc, CAP>(patch, s, T, G.acc, kp.gy);
             } else {
                 perr |= kErrLeftArea;

@@ -25,7 +25,7 @@ static inline double pow2_floor(double x) { return std::ldexp(1.0, (int)std::flo
 template <class Real, class Acc>
 class EngineT final : public Engine {
     static constexpr int BT = 128;       // threads per CTA of the fused kernel
-    static constexpr int PPT = 4;        // points per thread of the fused kernel
+    static constexpr int PPT = ICEMPM_FUSED_PPT;   // points per thread of the fused kernel
     static constexpr int CAP = 1024;     // nodes in the shared scatter tile
     static constexpr int BT_P2G = 256;   // threads per CTA of the priming scatter
     static constexpr int GRAPH_STEPS = 32;
@@ -72,6 +72,7 @@ public:
         ICEMPM_CUDA(cudaMalloc(&acc_, G_ * sizeof(Acc4<Acc>)));
         ICEMPM_CUDA(cudaMalloc(&vel_, G_ * sizeof(V2<Real>)));
         ICEMPM_CUDA(cudaMalloc(&cur_, G_ * sizeof(V2<Real>)));
+        ICEMPM_CUDA(cudaMalloc(&frc_, G_ * sizeof(V4<Real>)));
         ICEMPM_CUDA(cudaMalloc(&status_, G_));
         ICEMPM_CUDA(cudaMalloc(&force_, G_ * sizeof(double2)));
         ICEMPM_CUDA(cudaMalloc(&st_, sizeof(DevStatus)));
@@ -96,7 +97,7 @@ public:
         sort_tmp_bytes_ = std::max(t32, t64);
         ICEMPM_CUDA(cudaMalloc(&sort_tmp_, sort_tmp_bytes_));
         // a CTA of the fused kernel handles BT*PPT points, ~BT*PPT/4 cells at
-        // 4 points per cell: 8 columns of 16 cells
+        // 4 points per cell: 8 columns of BT*PPT/32 cells
         tile_.tx = 8; tile_.ty = BT * PPT / 32;
         tile_.ntiles_y = (gy_ + tile_.ty - 1) / tile_.ty;
         return set_params(p, 1.0);
@@ -109,7 +110,7 @@ public:
         KParams<Real> &k = kp_;
         k.gx = gx_; k.gy = gy_;
         k.update_every = p.UpdateEveryNthStep;
-        k.ext = opts_.forcing == ICEMPM_FORCING_EXTENDED; k.wind_kind = opts_.wind_kind;
+        k.ext = opts_.forcing == ICEMPM_FORCING_EXTENDED; k.wind_kind = opts_.wind_kind;   // wind lives in frc_
         k.h = Real(p.cellsize); k.h_inv = Real(p.cellsize_inv);
         k.dt = Real(p.InitialTimeStep);
         k.dt_h_inv = Real(p.InitialTimeStep * p.cellsize_inv);
@@ -129,10 +130,6 @@ public:
         k.lim_p = (float)(std::ldexp(1.0, 56) / k.scale_p);
         k.ext_impulse = Real(p.InitialTimeStep * p.ParticleVolume);
         k.rho_w_cd = Real(opts_.water_density * opts_.water_drag_coeff);
-        k.rho_a_ca = Real(opts_.air_density * opts_.air_drag_coeff);
-        k.wind_u = Real(opts_.wind_u); k.wind_v = Real(opts_.wind_v);
-        k.wind_cx = Real(opts_.wind_cx); k.wind_cy = Real(opts_.wind_cy);
-        k.wind_vmax = Real(opts_.wind_vmax); k.wind_radius = Real(opts_.wind_radius);
         Material &m = k.mat;
         m.mu = p.mu; m.kappa = p.kappa; m.DP_threshold_p = p.DP_threshold_p;
         m.pmax = p.IceCompressiveStrength; m.pmin = -p.IceTensileStrength;
@@ -146,14 +143,41 @@ public:
         return 0;
     }
 
+    // Wind at a world position for the extended forcing: uniform, or a
+    // Rankine vortex (solid-body inside the radius, 1/r outside).
+    void wind(double x, double y, double &ux, double &uy) const
+    {
+        ux = 0; uy = 0;
+        if (opts_.wind_kind == ICEMPM_WIND_UNIFORM) { ux = opts_.wind_u; uy = opts_.wind_v; }
+        else if (opts_.wind_kind == ICEMPM_WIND_RANKINE) {
+            const double dx = x - opts_.wind_cx, dy = y - opts_.wind_cy;
+            const double r = std::sqrt(dx * dx + dy * dy);
+            if (r > 0) {
+                const double sp = (r < opts_.wind_radius) ? opts_.wind_vmax * r / opts_.wind_radius
+                                                          : opts_.wind_vmax * opts_.wind_radius / r;
+                ux = -dy / r * sp; uy = dx / r * sp;
+            }
+        }
+    }
+
+    // Current per node, and for the extended forcing the node table
+    // {current, wind stress rho_a Ca |U| U} read by the point impulses.
     int set_current(const double *cur) override
     {
         std::vector<V2<Real>> h(G_);
+        std::vector<V4<Real>> f(G_);
+        const double ca = opts_.air_density * opts_.air_drag_coeff;
         for (size_t i = 0; i < G_; i++) {
-            h[i].x = cur ? Real(cur[i]) : Real(0);
-            h[i].y = cur ? Real(cur[G_ + i]) : Real(0);
+            const double cx = cur ? cur[i] : 0.0, cy = cur ? cur[G_ + i] : 0.0;
+            h[i].x = Real(cx); h[i].y = Real(cy);
+            double ux, uy;
+            wind((double)(i / gy_) * prms_.cellsize, (double)(i % gy_) * prms_.cellsize, ux, uy);
+            const double um = std::sqrt(ux * ux + uy * uy);
+            f[i].x = Real(cx); f[i].y = Real(cy);
+            f[i].z = Real(ca * um * ux); f[i].w = Real(ca * um * uy);
         }
         ICEMPM_CUDA(cudaMemcpyAsync(cur_, h.data(), G_ * sizeof(V2<Real>), cudaMemcpyHostToDevice, stream_));
+        ICEMPM_CUDA(cudaMemcpyAsync(frc_, f.data(), G_ * sizeof(V4<Real>), cudaMemcpyHostToDevice, stream_));
         ICEMPM_CUDA(cudaStreamSynchronize(stream_));
         return 0;
     }
@@ -458,7 +482,7 @@ private:
     Grid<Real, Acc> grid() const
     {
         Grid<Real, Acc> g;
-        g.acc = acc_; g.vel = vel_; g.cur = cur_; g.status = status_; g.force = force_;
+        g.acc = acc_; g.vel = vel_; g.cur = cur_; g.frc = frc_; g.status = status_; g.force = force_;
         return g;
     }
     void invalidate_graphs()
@@ -469,7 +493,7 @@ private:
     {
         if (stream_) cudaStreamSynchronize(stream_);
         invalidate_graphs();
-        cudaFree(pts_mem_); cudaFree(acc_); cudaFree(vel_); cudaFree(cur_); cudaFree(status_);
+        cudaFree(pts_mem_); cudaFree(acc_); cudaFree(vel_); cudaFree(cur_); cudaFree(frc_); cudaFree(status_);
         cudaFree(force_); cudaFree(st_); cudaFree(stage_); cudaFree(keys_[0]); cudaFree(keys_[1]);
         cudaFree(vals_[0]); cudaFree(vals_[1]); cudaFree(sort_tmp_);
         if (ev0_) cudaEventDestroy(ev0_);
@@ -492,6 +516,7 @@ private:
     int par_ = 0;
     Acc4<Acc> *acc_ = nullptr;
     V2<Real> *vel_ = nullptr, *cur_ = nullptr;
+    V4<Real> *frc_ = nullptr;
     uint8_t *status_ = nullptr;
     double2 *force_ = nullptr;
     DevStatus *st_ = nullptr;

@@ -350,11 +350,12 @@ static uint32_t p2g_point(const SP *p, const double *soa, size_t pitch, size_t i
     for (int k = 0; k < 4; k++) sub[k] = particle_mass * Bp[k] - sc * PFt[k];
 
     /* extended forcing: impulse of the wind and water stresses over the
-       point's area during the step, distributed with the B-spline weights */
+       point's area during the step, distributed with the B-spline weights;
+       wind and current are taken at the point's cell node */
     double fx = 0, fy = 0;
     if (ext) {
         double ux, uy;
-        wind_at(ext, (cx + pos[0]) * h, (cy + pos[1]) * h, &ux, &uy);
+        wind_at(ext, cx * h, cy * h, &ux, &uy);   /* wind sampled at the point's cell node */
         const double um = sqrt(ux * ux + uy * uy);
         const long long nc = (long long)cy + (long long)cx * gridY;
         double wx = 0, wy = 0;

@@ -19,7 +19,7 @@ EXPORTS = [
     "icempm_get_status", "icempm_clear_force_accumulator", "icempm_get_boundary_forces",
     "icempm_sort_compact", "icempm_timings", "icempm_phase_times", "icempm_fixed_point_scales",
     "icempm_host_register", "icempm_host_unregister", "icempm_device_count", "icempm_point_count",
-    "icempm_get_stream", "icempm_launch_count", "icempm_last_error",
+    "icempm_get_stream", "icempm_launch_count", "icempm_last_error", "icempm_cell_order_noalloc",
 ]
 
 
@@ -66,6 +66,8 @@ def load(path: str = LIB_PATH):
         "icempm_get_stream": (C.c_int, [h, C.POINTER(C.c_void_p)]),
         "icempm_launch_count": (C.c_int, [h, C.POINTER(C.c_uint64)]),
         "icempm_last_error": (C.c_char_p, []),
+        "icempm_cell_order_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_int32,
+                                                C.c_void_p, C.c_void_p, C.c_void_p]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -262,6 +262,27 @@ ICEMPM_API int icempm_get_stream(icempm_t *ctx, void **stream);
 /* Number of kernel launches this context has enqueued since creation. */
 ICEMPM_API int icempm_launch_count(icempm_t *ctx, uint64_t *count);
 
+/* Largest point count icempm_cell_order_noalloc accepts. */
+#define ICEMPM_NOALLOC_MAX_POINTS (1u << 20)
+
+/* Compaction order without device allocation.  No counterpart in the
+ * reference.  For callers that must not allocate device memory -- code whose
+ * host framework owns every device byte through its own pool, or that issues
+ * work into a stream it cannot synchronise around cudaMalloc/cudaFree -- this
+ * computes the order icempm_sort_compact applies: d_order[0..*d_count) are the
+ * indices of the points without ICEMPM_STATUS_DISABLED, sorted by cell index
+ * x*grid_y + y of the cell word d_cell[i] ((y << 16) | x), ties in index
+ * order.  Inputs d_cell, d_utility (n words each) and outputs d_order (n
+ * words) and d_count (1 word) are the caller's device buffers.  All
+ * intermediate storage is one static device array of 36 MiB that every GPU
+ * loading this library keeps until exit; n above ICEMPM_NOALLOC_MAX_POINTS is
+ * rejected with ICEMPM_E_CAPACITY.  The first call on a device resolves that
+ * array's address (set-up), so make it before any stream capture.  Calls share
+ * the array: calls that overlap on the GPU race.  Asynchronous on `stream`
+ * (cudaStream_t, NULL = default stream); allocates nothing. */
+ICEMPM_API int icempm_cell_order_noalloc(const uint32_t *d_cell, const uint32_t *d_utility, uint32_t n,
+                                         int32_t grid_y, uint32_t *d_order, uint32_t *d_count, void *stream);
+
 /* Message of the last failing call on this thread ("" if none). */
 ICEMPM_API const char *icempm_last_error(void);
 

@@ -17,6 +17,11 @@ oracle on the host cores.  Under torchrun every rank runs its own scene
 (different seed: weak scaling, no collective in the step); rank 0 prints one
 JSON line with the whole-job throughput (max time over ranks).
 
+Beside them, on rank 0 at N=1: the reference's own CUDA step
+(simulation/kernels.cuh compiled for sm_100a in oracle/_ref, single
+partition, FP64, its own launch shapes) on the same scene, timed with CUDA
+events around its sub-step loop ("reference_gpu").
+
 --impl reference: the reference's own kernels (simulation/kernels.cuh,
 compiled for the host in oracle/_ref) advance a bounded sample of the same
 scene family on the host cores; rank 0 only.
@@ -60,6 +65,8 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=4)
+    ap.add_argument("--no-ref-gpu", action="store_true")
+    ap.add_argument("--ref-gpu-steps", type=int, default=50)
     ap.add_argument("--grid", type=int, nargs=2, default=None, metavar=("GX", "GY"),
                     help="same scene rules on a smaller GX x GY grid (seeds scaled by area), "
                          "for profiling captures")
@@ -172,6 +179,33 @@ def run_reference(args, rank):
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample, "note": note},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def reference_gpu_baseline(args, sc):
+    """The reference's CUDA step on the benchmark scene: memset of grid rows
+    0-2, partition_kernel_p2g, partition_kernel_update_nodes and
+    partition_kernel_g2p per sub-step (gpu_partition.cpp:300-365), timed with
+    CUDA events around the loop after warm-up.  The reference has no wind
+    term: it runs the current-drag forcing of its update kernel."""
+    try:
+        from oracle.refbuild import build_ref_gpu
+        build_ref_gpu.load()
+    except (FileNotFoundError, OSError) as e:
+        return {"unavailable": "reference GPU library not built: %s" % e}
+    G = sc.grid_nodes
+    grid = np.zeros((9, G))
+    grid[5], grid[6] = sc.current[:G], sc.current[G:2 * G]
+    k = max(1, args.ref_gpu_steps)
+    with build_ref_gpu.RefGpuScene(sc.prms, sc.status, grid, sc.n) as s:
+        s.upload(sc.soa, sc.n)
+        s.run(max(3, args.warmup), 0)
+        ms = s.run(k, max(3, args.warmup))
+        err, _ = s.download(np.zeros((19, sc.n)))
+    return {"value": sc.n * k / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms / k, "steps": k, "dtype": "f64",
+            "device_errors": err,
+            "note": "reference simulation/kernels.cuh built for sm_100a (oracle/_ref/libicempm_ref_gpu.so), "
+                    "single partition, tpb P2G/update/G2P = %d/%d/%d, current-drag forcing only"
+                    % (sc.prms.tpb_P2G, sc.prms.tpb_Upd, sc.prms.tpb_G2P)}
 
 
 def cpu_baseline(args, sc):
@@ -287,6 +321,9 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(args, sc)
+    ref_gpu = None
+    if rank == 0 and world == 1 and not args.no_ref_gpu:
+        ref_gpu = reference_gpu_baseline(args, sc)
 
     if rank == 0:
         workload = WORKLOAD if args.grid is None else WORKLOAD.replace("4096x2048", "%dx%d" % tuple(args.grid))
@@ -300,7 +337,7 @@ def main():
                            "parallelism": f"{world} independent scene(s), one per GPU",
                            "l2": "inputs larger than L2 (2.0 GB point state, 0.4 GB grid)",
                            "device_errors": err},
-                "plain": plain, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+                "plain": plain, "reference_gpu": ref_gpu, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
                 "gpu_launches": launches, "clocks": clocks}
         print(json.dumps(line), flush=True)
     if dist:

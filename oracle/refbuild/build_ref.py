@@ -6,8 +6,9 @@ Compiles ref_harness.cpp (which #includes simulation/kernels.cuh,
 helper_math.cuh, givens.cuh and parameters_sim.h where they lie) together
 with simulation/parameters_sim.cpp, hssoa/host_side_soa.cpp and
 hssoa/proxypoint2d.cpp, all read in place from the reference checkout, with
-g++ and the stand-in headers in oracle/refbuild/stubs (CUDA qualifiers and
-atomics, spdlog/fmt/HDF5 no-ops, a 2x2 subset of the Eigen API).  Needs the
+g++ and the stand-in headers in oracle/refbuild/stubs_host (CUDA qualifiers and
+atomics for a host build) and oracle/refbuild/stubs (spdlog/fmt/HDF5
+no-ops, a 2x2 subset of the Eigen API).  Needs the
 reference checkout, so it runs only where the checkout exists; the built
 library travels with the repository snapshot.  TEST INFRASTRUCTURE ONLY.
 """
@@ -36,12 +37,12 @@ def build(force: bool = False) -> str:
             os.path.join(sim, "parameters_sim.cpp"),
             os.path.join(sim, "hssoa", "host_side_soa.cpp"),
             os.path.join(sim, "hssoa", "proxypoint2d.cpp")]
-    deps = srcs + [os.path.join(HERE, "stubs", "Eigen", "Core"), os.path.join(HERE, "stubs", "cuda_runtime.h")]
+    deps = srcs + [os.path.join(HERE, "stubs", "Eigen", "Core"), os.path.join(HERE, "stubs_host", "cuda_runtime.h")]
     if not force and os.path.exists(LIB) and all(os.path.getmtime(LIB) >= os.path.getmtime(d) for d in deps):
         return LIB
     os.makedirs(OUT_DIR, exist_ok=True)
     cmd = ["g++", "-std=c++20", "-O2", "-fopenmp", "-ffp-contract=off", "-fPIC", "-shared", "-w",
-           "-I", os.path.join(HERE, "stubs"),
+           "-I", os.path.join(HERE, "stubs_host"), "-I", os.path.join(HERE, "stubs"),
            "-I", sim, "-I", os.path.join(sim, "hssoa"),
            "-I", os.path.join(REF, "External"),
            "-o", LIB] + srcs

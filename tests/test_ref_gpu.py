@@ -1,0 +1,103 @@
+"""The reference's own CUDA step (simulation/kernels.cuh compiled for sm_100a by
+oracle/refbuild/build_ref_gpu.py) on the GPU: first pinned against the golden
+fixtures, then used as the expected value for the B200 step on scenes too
+large for the host reference.
+
+Tolerances (parity_util.errors):
+  * reference GPU step vs the golden fixtures (same kernels on the host, FMA
+    contraction off, P2G in index order): 1e-9 after up to 60 steps, 1e-4 on
+    the chaotic disable_then_sort fixture -- what separates them is FP64
+    summation order (atomics) and FMA contraction.
+  * B200 FP64 variant vs the reference GPU step, 20 steps of a 76k-point
+    Voronoi scene: 1e-9; identical flags, cell keys and error word.
+  * B200 fixed-point and FP32 variants: world position <= 1e-5 relative and
+    velocity <= 1e-5 relative after one step; after 20 steps position
+    <= 1e-4 cells, velocity <= 1e-3, at most 1% of points with a different
+    crushed latch or cell key.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from icempm_2d_sp_b200 import scenes
+from icempm_2d_sp_b200.params import SimParams, Options
+from parity_util import errors
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+FIXTURES = ["random_1step", "random_10step", "random_plastic_20step", "ridging_60step", "disable_then_sort"]
+
+
+@pytest.fixture(scope="module")
+def ref_gpu():
+    from oracle.refbuild import build_ref_gpu
+    L = build_ref_gpu.load()
+    if L.ref_gpu_device_count() < 1:
+        pytest.fail("no CUDA device visible to the reference GPU library")
+    return build_ref_gpu
+
+
+def grid_rows(prms, current):
+    G = prms.GridXTotal * prms.GridYTotal
+    g = np.zeros((9, G))
+    g[5], g[6] = current[:G], current[G:2 * G]
+    return g
+
+
+def run_reference_gpu(ref_gpu, prms, status, current, soa_in, n, nsteps, first_step):
+    out = np.zeros_like(soa_in)
+    with ref_gpu.RefGpuScene(prms, status, grid_rows(prms, current), soa_in.shape[1]) as s:
+        s.upload(soa_in, n)
+        s.run(nsteps, first_step)
+        err, dis = s.download(out)
+    return out, err, dis
+
+
+@pytest.mark.parametrize("name", FIXTURES)
+def test_reference_gpu_step_matches_golden(ref_gpu, name):
+    z = np.load(os.path.join(GOLDEN, name + ".npz"))
+    prms = SimParams.from_buffer_copy(z["prms"].tobytes())
+    n = int(z["n"])
+    out, err, dis = run_reference_gpu(ref_gpu, prms, z["status"], z["current"], z["soa_in"], n,
+                                      int(z["nsteps"]), int(z["first_step"]))
+    e = errors(out, z["soa_out"], n, prms.cellsize)
+    tol = 1e-4 if name == "disable_then_sort" else 1e-9
+    assert err == int(z["err"]) and dis == int(z["disabled"])
+    assert e["pid_equal"] and e["thickness_equal"] and e["flags_mismatch"] == 0 and e["cell_mismatch"] == 0, e
+    assert e["pos_cells"] < tol and e["vel_rel"] < tol and e["fe_abs"] < tol, e
+
+
+@pytest.fixture(scope="module")
+def voronoi_scene():
+    # config1 generation rules on a 256x128 grid (76k points); the reference
+    # has no wind term, so both sides run the reference's forcing
+    return scenes.config1(seed=77, gx=256, gy=128, n_seeds=8)
+
+
+@pytest.mark.parametrize("nsteps", [1, 20])
+@pytest.mark.parametrize("variant", ["fixed", "fp32", "fp64"])
+def test_b200_step_matches_reference_gpu_step(ref_gpu, voronoi_scene, variant, nsteps):
+    from icempm_2d_sp_b200 import capi
+    sc = voronoi_scene
+    ref, rerr, rdis = run_reference_gpu(ref_gpu, sc.prms, sc.status, sc.current, sc.soa, sc.n, nsteps, 0)
+    with capi.Context(sc.prms, sc.status, sc.current, capacity=sc.soa.shape[1],
+                      options=Options.default(variant=variant)) as ctx:
+        ctx.upload(sc.soa, sc.n)
+        ctx.step(nsteps, 0)
+        out, m = ctx.download(np.zeros_like(sc.soa))
+        err, dis = ctx.status()
+    assert m == sc.n and err == rerr
+    e = errors(out, ref, sc.n, sc.prms.cellsize)
+    assert e["pid_equal"] and e["thickness_equal"]
+    if variant == "fp64":
+        assert dis == rdis and e["flags_mismatch"] == 0 and e["cell_mismatch"] == 0, e
+        assert e["pos_cells"] < 1e-9 and e["vel_rel"] < 1e-9 and e["fe_abs"] < 1e-9, e
+    elif nsteps == 1:
+        assert dis == rdis and e["flags_mismatch"] == 0 and e["cell_mismatch"] == 0, e
+        assert e["pos_rel"] <= 1e-5 and e["vel_rel"] <= 1e-5 and e["fe_abs"] <= 1e-6, e
+    else:
+        lim = max(1, sc.n // 100)
+        assert abs(dis - rdis) <= lim and e["flags_mismatch"] <= lim and e["cell_mismatch"] <= lim, e
+        assert e["pos_cells"] <= 1e-4 and e["vel_rel"] <= 1e-3 and e["fe_abs"] <= 1e-5, e

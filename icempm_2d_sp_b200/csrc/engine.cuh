@@ -18,8 +18,13 @@
 //   A   {x, y, Jp_inv, thickness}  x, y cell-local in [-0.5, 0.5]
 //   H   {H00, H01, H10, H11}       H = Fe - I
 //   K   {cell, utility}            cell = (y << 16) | x, utility flags
-//   V   {vx, vy}                   written each step, read only when priming
+//   V   {vx, vy}                   read only when priming
 //   C   {C00, C01, C10, C11}       APIC affine matrix (the reference's Bp)
+// The fused kernel hands V and C from its G2P to its P2G in registers, so
+// between the sub-steps of one icempm_step call they are dead: they are
+// stored by the call's last sub-step (DevStatus::vc_step) and by the sub-step
+// that disables a point (its last), which leaves the state after the call
+// identical to storing them every sub-step.
 //   PQ  {P, Q}                     written on record steps only
 //   slot, pid, thick64             host slot, point id row, f64 thickness
 // Grid layout (node = y + x*GridY, the reference order):
@@ -95,7 +100,8 @@ struct DevStatus {
     uint32_t done;         // CTA completion ticket of the fused kernel
     int32_t n_active;      // result slot of the compaction boundary search
     uint32_t err_pending;  // bits of the scatter for the next sub-step
-    int32_t pad[2];
+    int32_t vc_step;       // G2P sub-step whose point velocity and C are stored
+    int32_t pad;
 };
 
 template <class Real> struct Pts {
@@ -554,6 +560,7 @@ k_g2p_p2g(KParams<Real> kp, Pts<Real> P, Grid<Real, Acc> G, DevStatus *st, int n
 
     const int step = st->step;
     const bool recordPQ = kp.update_every > 0 && (step % kp.update_every) == 0;
+    const bool store_vc = step == st->vc_step;
     uint32_t err = 0, perr = 0;
     int ndis = 0;
     Patch<Real> patch;
@@ -655,10 +662,12 @@ k_g2p_p2g(KParams<Real> kp, Pts<Real> P, Grid<Real, Acc> G, DevStatus *st, int n
         st_stream(P.A + i, Ao);
         V4<Real> Ho; Ho.x = H.a00; Ho.y = H.a01; Ho.z = H.a10; Ho.w = H.a11;
         st_stream(P.H + i, Ho);
-        V2<Real> Vo; Vo.x = vx; Vo.y = vy;
-        st_stream(P.V + i, Vo);
-        V4<Real> Co; Co.x = c00; Co.y = c01; Co.z = c10; Co.w = c11;
-        st_stream(P.C + i, Co);
+        if (store_vc || (util & kDisabled)) {   // a point disabled now keeps this step's V and C
+            V2<Real> Vo; Vo.x = vx; Vo.y = vy;
+            st_stream(P.V + i, Vo);
+            V4<Real> Co; Co.x = c00; Co.y = c01; Co.z = c10; Co.w = c11;
+            st_stream(P.C + i, Co);
+        }
         const uint32_t cell = ((uint32_t)cy << 16) | (uint32_t)cx;   // as kernels.cuh:305
         if (moved || util != key.y) {
             uint2 ko; ko.x = moved ? cell : key.x; ko.y = util;

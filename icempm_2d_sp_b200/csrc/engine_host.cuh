@@ -314,7 +314,7 @@ public:
     {
         if (nsteps < 0) return fail(ICEMPM_E_ARG, "nsteps < 0");
         ICEMPM_CUDA(cudaEventRecord(ev0_, stream_));
-        k_set_step<<<1, 1, 0, stream_>>>(st_, first_step, 1);
+        k_set_step<<<1, 1, 0, stream_>>>(st_, first_step, 1, nsteps);
         launches_++;
         int rc = 0;
         if (!primed_) { rc = prime(); if (rc) return rc; }
@@ -366,6 +366,8 @@ public:
     {
         // time nsteps steps launched directly, accumulating per-kernel event pairs
         if (!primed_) { int rc = prime(); if (rc) return rc; }
+        k_set_step<<<1, 1, 0, stream_>>>(st_, -1, 0, nsteps);
+        launches_++;
         std::vector<cudaEvent_t> ev(3 * nsteps);
         for (auto &e : ev) ICEMPM_CUDA(cudaEventCreate(&e));
         ICEMPM_CUDA(cudaEventRecord(ev0_, stream_));

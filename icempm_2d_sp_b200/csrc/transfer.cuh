@@ -126,9 +126,13 @@ static __global__ void k_count_active(const uint64_t *__restrict__ keys, int n, 
     if (i == 0 && !act) st->n_active = 0;
 }
 
-static __global__ void k_set_step(DevStatus *st, int step, int reset_done)
+// Sets the index of the next sub-step (step >= 0; step < 0 keeps it) and
+// marks the last G2P sub-step of the coming nsteps as the one that stores
+// the point velocity and C.
+static __global__ void k_set_step(DevStatus *st, int step, int reset_done, int nsteps)
 {
-    st->step = step;
+    if (step >= 0) st->step = step;
+    st->vc_step = st->step + nsteps - 1;
     if (reset_done) st->done = 0;
 }
 

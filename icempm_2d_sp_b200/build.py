@@ -20,7 +20,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fvisibility=hidden",
          "--expt-relaxed-constexpr", "-I", os.path.join(ROOT, "include")]
-# developer knob for tuning builds, e.g. ICEMPM_EXTRA_FLAGS="-DICEMPM_FUSED_MINB=3"
+# developer knob for tuning builds, e.g. ICEMPM_EXTRA_FLAGS="-maxrregcount=96"
 FLAGS += os.environ.get("ICEMPM_EXTRA_FLAGS", "").split()
 SOURCES = ["capi.cu", "engine_fixed.cu", "engine_fp32.cu", "engine_fp64.cu", "noalloc.cu"]
 # The FP32-state engines use approximate single-precision division and square

@@ -10,6 +10,7 @@
 // each function equals its reference counterpart (cited per function,
 // simulation/kernels.cuh, helper_math.cuh, givens.cuh of igorg520b/iceMPM_2d_sp).
 #pragma once
+#include <cmath>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -20,7 +21,7 @@ constexpr uint32_t kDisabled = 0x20000u;
 constexpr uint32_t kErrPosNan = 0x0001u, kErrVelNan = 0x0002u, kErrJump = 0x0004u,
                    kErrLeftArea = 0x0008u, kErrBpNan = 0x0010u, kErrFeNan = 0x0020u,
                    kErrP2gNanVel = 0x0100u, kErrP2gNanMass = 0x0200u, kErrGridNan = 0x0400u,
-                   kErrFixedOverflow = 0x1000u;
+                   kErrFixedOverflow = 0x1000u, kErrBarrierTimeout = 0x2000u;
 
 template <class T> struct M2 { T a00, a01, a10, a11; };
 
@@ -158,20 +159,43 @@ struct Material {
     double mu, kappa, DP_threshold_p, pmin, pmax, qmax, pmin2, beta, M_sq, tan_phi, ridge_coeff_g_rho;
 };
 
+// The material constants in the arithmetic type of the kernels, with the
+// combinations the yield tests use formed once on the host in FP64.
+template <class T> struct MatT {
+    T mu, kappa, thr, pmin, pmax, qmax, pmin2, tan_phi, ridge;
+    T one_2beta;   // 1 + 2 beta
+    T beta_pmax;   // beta pmax
+    T M_sq;
+    T cone_k;      // slope of the tension cone: -q0 / pmin2, q0 = 2 sqrt(-pmax pmin) qmax / (pmax - pmin)
+    T fs_c;        // 2 qmax / (pmax - pmin) of the elliptic failure surface
+};
+
+template <class T> inline MatT<T> mat_of(const Material &m)
+{
+    MatT<T> r;
+    r.mu = T(m.mu); r.kappa = T(m.kappa); r.thr = T(m.DP_threshold_p);
+    r.pmin = T(m.pmin); r.pmax = T(m.pmax); r.qmax = T(m.qmax); r.pmin2 = T(m.pmin2);
+    r.tan_phi = T(m.tan_phi); r.ridge = T(m.ridge_coeff_g_rho);
+    r.one_2beta = T(1.0 + 2.0 * m.beta);
+    r.beta_pmax = T(m.beta * m.pmax);
+    r.M_sq = T(m.M_sq);
+    const double q0 = 2.0 * std::sqrt(-m.pmax * m.pmin) * m.qmax / (m.pmax - m.pmin);
+    r.cone_k = T(-q0 / m.pmin2);
+    r.fs_c = T(2.0 * m.qmax / (m.pmax - m.pmin));
+    return r;
+}
+
 // One-way latch of the crushed flag (CheckIfPointIsInsideFailureSurface with
 // GetParametersForGrain, kernels.cuh:349-369,538-566).
 template <class T>
-__device__ __forceinline__ uint32_t failure_check(const Material &m, uint32_t util, T p, T q)
+__device__ __forceinline__ uint32_t failure_check(const MatT<T> &m, uint32_t util, T p, T q)
 {
-    const T pmin2 = T(m.pmin2), pmax = T(m.pmax);
     if (p < T(0)) {
-        if (p < pmin2) return util | kCrushed;
-        const T q0 = T(2) * tsqrt(T(-m.pmax * m.pmin)) * T(m.qmax) / T(m.pmax - m.pmin);
-        const T k = -q0 / pmin2;
-        const T q_limit = k * (p - pmin2);
+        if (p < m.pmin2) return util | kCrushed;
+        const T q_limit = m.cone_k * (p - m.pmin2);
         if (q > q_limit) return util | kCrushed;
     } else {
-        const T y = (T(1) + T(2) * T(m.beta)) * q * q + T(m.M_sq) * (p + T(m.beta) * pmax) * (p - pmax);
+        const T y = m.one_2beta * q * q + m.M_sq * (p + m.beta_pmax) * (p - m.pmax);
         if (y > T(0)) return util | kCrushed;
     }
     return util;
@@ -180,13 +204,13 @@ __device__ __forceinline__ uint32_t failure_check(const Material &m, uint32_t ut
 // Drucker-Prager / Wolper return map on H (Wolper_Drucker_Prager, kernels.cuh:374-483).
 // The plastic volume ratio Jp_inv is updated in FP64.
 template <class T>
-__device__ __forceinline__ void wolper_dp(const Material &m, T thickness, T p_tr, T q_tr, const Kin<T> &k,
+__device__ __forceinline__ void wolper_dp(const MatT<T> &m, T thickness, T p_tr, T q_tr, const Kin<T> &k,
                                           const SvdH<T> &sv, M2<T> &H, T &Jp_inv)
 {
-    const T mu = T(m.mu), kappa = T(m.kappa);
-    const T thr = T(m.DP_threshold_p);
-    const T pmin = T(m.pmin), pmax = T(m.pmax), qmax = T(m.qmax);
-    const T tan_phi = T(m.tan_phi);
+    const T mu = m.mu, kappa = m.kappa;
+    const T thr = m.thr;
+    const T pmin = m.pmin, pmax = m.pmax;
+    const T tan_phi = m.tan_phi;
     if (p_tr < thr) {
         if (Jp_inv < T(0.1)) {                       // case 0: Fe = sqrt(J) U V^T
             const T a = sqrt1pm1(k.Jm1);
@@ -199,7 +223,7 @@ __device__ __forceinline__ void wolper_dp(const Material &m, T thickness, T p_tr
     }
     T q_yield;
     if (p_tr < pmax) {
-        const T q_fs = T(2) * tsqrt((pmax - p_tr) * (p_tr - pmin)) * qmax / (pmax - pmin);
+        const T q_fs = m.fs_c * tsqrt((pmax - p_tr) * (p_tr - pmin));
         const T q_dp = fmax(T(0), (p_tr - thr) * tan_phi);
         q_yield = fmin(q_fs, q_dp);
     } else {
@@ -207,12 +231,12 @@ __device__ __forceinline__ void wolper_dp(const Material &m, T thickness, T p_tr
     }
     if (!(q_tr > q_yield)) return;                   // case 2: elastic
     // case 3: project onto the yield surface
-    const T p_ridge_max = T(m.ridge_coeff_g_rho) * thickness * Jp_inv;
+    const T p_ridge_max = m.ridge * thickness * Jp_inv;
     const T p_n_1 = fmin(p_tr, p_ridge_max);
     T q_n_1;
     if (p_n_1 < pmax) {
         const T q_dp = fmax(T(0), (p_n_1 - thr) * tan_phi);
-        const T q_fs = T(2) * tsqrt((pmax - p_n_1) * (p_n_1 - pmin)) * qmax / (pmax - pmin);
+        const T q_fs = m.fs_c * tsqrt((pmax - p_n_1) * (p_n_1 - pmin));
         q_n_1 = fmin(q_fs, q_dp);
     } else {
         q_n_1 = T(0);

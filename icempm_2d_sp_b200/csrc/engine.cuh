@@ -40,15 +40,32 @@
 #include <cub/device/device_radix_sort.cuh>
 
 #include "device_math.cuh"
-#include "../../include/icempm.h"
+#include "icempm.h"
 
-// CTAs per SM the fused kernel is compiled for (FP32 state; FP64 keeps 1),
-// and points per thread of the fused kernel.
+// Shape of the FP32-state fused kernel: threads per CTA, points per thread,
+// nodes of the shared scatter tile, CTAs per SM it is compiled for (this
+// caps registers at 96: occupancy is what hides its latencies).
+#ifndef ICEMPM_FUSED_BT
+#define ICEMPM_FUSED_BT 128
+#endif
+#ifndef ICEMPM_FUSED_PPT
+#define ICEMPM_FUSED_PPT 4
+#endif
+#ifndef ICEMPM_FUSED_CAP
+#define ICEMPM_FUSED_CAP 512
+#endif
 #ifndef ICEMPM_FUSED_MINB
 #define ICEMPM_FUSED_MINB 5
 #endif
-#ifndef ICEMPM_FUSED_PPT
-#define ICEMPM_FUSED_PPT 8
+// Stages of point state in shared memory (2: the next chunk is fetched while
+// this one is computed; 1: it is fetched while this one's tile is flushed,
+// which leaves room for more CTAs per SM).
+#ifndef ICEMPM_FUSED_STAGES
+#define ICEMPM_FUSED_STAGES 1
+#endif
+// 1: persistent grid of as many CTAs as fit; 0: one CTA per chunk.
+#ifndef ICEMPM_FUSED_PERSIST
+#define ICEMPM_FUSED_PERSIST 1
 #endif
 
 namespace icempm {
@@ -133,7 +150,7 @@ template <class Real> struct KParams {
     float lim_m, lim_p;             // largest |value| a single term may carry in fixed point
     Real ext_impulse;               // dt * ParticleVolume (extended forcing)
     Real rho_w_cd;                  // rho_w * Cd (extended forcing)
-    Material mat;
+    MatT<Real> mat;
 };
 
 // ---- accumulator conversions -------------------------------------------
@@ -200,19 +217,18 @@ template <class Real> struct Src {
 };
 
 template <class Real, class Acc>
-__device__ __forceinline__ void make_src(const KParams<Real> &kp, const V4<Real> *__restrict__ frc, Src<Real> &s,
+__device__ __forceinline__ void make_src(const KParams<Real> &kp, const V4<Real> &f, Src<Real> &s,
                                          Real x, Real y, Real Jp, Real thick, const Kin<Real> &k, Real vx,
                                          Real vy, Real c00, Real c01, Real c10, Real c11, uint32_t &perr)
 {
-    const M2<Real> tau = kirchhoff(k, Real(kp.mat.mu), Real(kp.mat.kappa));
+    const M2<Real> tau = kirchhoff(k, kp.mat.mu, kp.mat.kappa);
     const Real mp = kp.particle_mass * thick;
     const Real sc = kp.dt_vol_Dpinv * Jp * thick;
     const Real S00 = mp * c00 - sc * tau.a00, S01 = mp * c01 - sc * tau.a01;
     const Real S10 = mp * c10 - sc * tau.a10, S11 = mp * c11 - sc * tau.a11;
     Real ax = mp * vx - kp.h * (S00 * x + S01 * y);
     Real ay = mp * vy - kp.h * (S10 * x + S11 * y);
-    if (kp.ext) {
-        const V4<Real> f = frc[(uint32_t)s.cx * (uint32_t)kp.gy + (uint32_t)s.cy];
+    if (kp.ext) {   // f = forcing entry of the point's cell node
         const Real dx = f.x - vx, dy = f.y - vy;
         const Real cw = kp.rho_w_cd * tsqrt(dx * dx + dy * dy);
         ax += kp.ext_impulse * (f.z + cw * dx);
@@ -250,8 +266,11 @@ __device__ __forceinline__ void src_terms(const Src<Real> &s, int a, int b, Real
 template <class Acc, int CAP> struct Tile {
     Acc (*t)[CAP];
     int x0, y0, tw, th;
+    unsigned th_rcp;   // ceil(2^32 / th): entry k lies in column umulhi(k, th_rcp) (exact while k * th < 2^32)
     bool on;
 };
+
+__device__ __forceinline__ unsigned rcp32(int d) { return d > 0 ? 0xffffffffu / (unsigned)d + 1u : 0u; }
 
 template <class Real, class Acc, int CAP>
 __device__ __forceinline__ void node_add(const Tile<Acc, CAP> &T, bool in_tile, Acc4<Acc> *__restrict__ gacc,
@@ -287,7 +306,7 @@ __device__ __forceinline__ void tile_flush(const Tile<Acc, CAP> &T, Acc4<Acc> *_
 {
     const int nt = T.tw * T.th;
     for (int k = threadIdx.x; k < nt; k += BT) {
-        const int lx = k / T.th, ly = k - lx * T.th;
+        const int lx = (int)__umulhi((unsigned)k, T.th_rcp), ly = k - lx * T.th;
         const int X = T.x0 + lx, Y = T.y0 + ly;
         const Acc m = T.t[0][k], px = T.t[1][k], py = T.t[2][k];
         if ((m != Acc(0) || px != Acc(0) || py != Acc(0)) && X >= 0 && X < gx && Y >= 0 && Y < gy) {
@@ -321,6 +340,7 @@ __device__ __forceinline__ Tile<Acc, CAP> make_tile(Acc (*t)[CAP], int *box, boo
     // 64-bit product: a box spanning the whole grid must not wrap into range
     T.on = box[2] >= 0 && (long long)T.tw * (long long)T.th <= (long long)CAP;
     if (!T.on) { T.tw = 0; T.th = 0; }
+    T.th_rcp = rcp32(T.th);
     return T;
 }
 
@@ -358,7 +378,9 @@ __global__ void __launch_bounds__(BT) k_p2g(KParams<Real> kp, Pts<Real> P, Grid<
                 const V4<Real> A = P.A[i], Hv = P.H[i], Cv = P.C[i];
                 const V2<Real> v = P.V[i];
                 const M2<Real> H = {Hv.x, Hv.y, Hv.z, Hv.w};
-                make_src<Real, Acc>(kp, G.frc, s, A.x, A.y, A.z, A.w, kinematics(H), v.x, v.y,
+                V4<Real> f{};
+                if (kp.ext) f = G.frc[(uint32_t)s.cx * (uint32_t)kp.gy + (uint32_t)s.cy];
+                make_src<Real, Acc>(kp, f, s, A.x, A.y, A.z, A.w, kinematics(H), v.x, v.y,
                                     Cv.x, Cv.y, Cv.z, Cv.w, perr);
                 active = true;
             } else {
@@ -458,6 +480,54 @@ template <int PPT> __host__ __device__ __forceinline__ uint32_t fused_index(uint
     return warp * (uint32_t)(32 * PPT) + (uint32_t)(j * 32 + lane);
 }
 
+// ---- bulk asynchronous copies into shared memory ----------------------------
+// cp.async.bulk (the TMA engine's 1D form) with an mbarrier that counts the
+// bytes in flight; waits are bounded in iterations and in time.
+__device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long *bar, uint32_t bytes)
+{
+    unsigned long long state;
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 %0, [%1], %2;"
+                 : "=l"(state) : "r"(smem_addr(bar)), "r"(bytes) : "memory");
+    (void)state;
+}
+__device__ __forceinline__ void bulk_to_smem(void *dst, const void *src, uint32_t bytes, unsigned long long *bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(smem_addr(dst)), "l"(src), "r"(bytes), "r"(smem_addr(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n}"
+                 : "=r"(ok) : "r"(smem_addr(bar)), "r"(parity) : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// Gives up after 2^24 polls or 1 s, whichever comes first.
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long *bar, uint32_t parity)
+{
+    if (mbar_try_wait(bar, parity)) return true;
+    const unsigned long long t0 = global_ns();
+    for (uint32_t k = 0; k < (1u << 24); k++) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if ((k & 255u) == 255u && global_ns() - t0 > 1000000000ull) return false;
+    }
+    return false;
+}
+
 // A thread accumulates its points' node terms in a register patch of the
 // 3x3 nodes around cell (cx, cy).  When the next point sits one cell higher
 // in the same column the patch slides: its lowest node row is written out and
@@ -477,6 +547,31 @@ __device__ __forceinline__ void patch_flush(Patch<Real> &p, const Tile<Acc, CAP>
         for (int b = 0; b < 3; b++)
             node_add<Real, Acc, CAP>(T, p.in_tile, gacc, gy, p.cx + a - 1, p.cy + b - 1, p.m[a][b], p.px[a][b], p.py[a][b]);
     p.have = false;
+}
+
+// The node terms of src_terms, summed separably: with
+//   u_a = m wx_a,  p_a = wx_a (ax + s00 (a-1)),  q_a = wx_a s01,
+//   r_a = wx_a (ay + s10 (a-1)),  t_a = wx_a s11,
+// node (a, b) receives  m: u_a wy_b,  px: wy_b (p_a + (b-1) q_a),  py: wy_b (r_a + (b-1) t_a).
+template <class Real> __device__ __forceinline__ void patch_accumulate(Patch<Real> &p, const Src<Real> &s)
+{
+    const Real axa[3] = {s.ax - s.s00, s.ax, s.ax + s.s00};
+    const Real aya[3] = {s.ay - s.s10, s.ay, s.ay + s.s10};
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        const Real u = s.mp * s.wx[a];
+        const Real pa = s.wx[a] * axa[a], qa = s.wx[a] * s.s01;
+        const Real ra = s.wx[a] * aya[a], ta = s.wx[a] * s.s11;
+        p.m[a][0] += u * s.wy[0];
+        p.m[a][1] += u * s.wy[1];
+        p.m[a][2] += u * s.wy[2];
+        p.px[a][0] += s.wy[0] * (pa - qa);
+        p.px[a][1] += s.wy[1] * pa;
+        p.px[a][2] += s.wy[2] * (pa + qa);
+        p.py[a][0] += s.wy[0] * (ra - ta);
+        p.py[a][1] += s.wy[1] * ra;
+        p.py[a][2] += s.wy[2] * (ra + ta);
+    }
 }
 
 template <class Real, class Acc, int CAP>
@@ -508,14 +603,36 @@ __device__ __forceinline__ void patch_add(Patch<Real> &p, const Src<Real> &s, co
         p.in_tile = cell_in_tile(T, s.cx, s.cy);
         p.have = true;
     }
-#pragma unroll
-    for (int a = 0; a < 3; a++)
-#pragma unroll
-        for (int b = 0; b < 3; b++) {
-            Real m, px, py;
-            src_terms(s, a, b, m, px, py);
-            p.m[a][b] += m; p.px[a][b] += px; p.py[a][b] += py;
-        }
+    patch_accumulate(p, s);
+}
+
+// Shared memory of one CTA of the fused kernel.  A chunk is CH = BT*PPT
+// consecutive points; the stages hold the point state of the current chunk
+// (and with two stages the next one), which the bulk copy engine fetches
+// ahead; `tile` holds the scatter accumulators of the chunk's cells +-2 nodes.
+template <class Real, class Acc, int BT, int PPT, int CAP, int STAGES> struct ChunkSmem {
+    static constexpr int CH = BT * PPT;
+    struct Stage {
+        V4<Real> A[CH];
+        V4<Real> H[CH];
+        uint2 K[CH];
+    };
+    Stage stage[STAGES];
+    Acc tile[3][CAP];
+    unsigned long long mbar[2];
+    int red[BT / 32][5];
+};
+
+template <class Real, class Stage>
+__device__ __forceinline__ void fetch_chunk(Stage &sg, const Pts<Real> &P, uint32_t base, int ch,
+                                            unsigned long long *bar)
+{
+    const uint32_t bv = (uint32_t)ch * (uint32_t)sizeof(V4<Real>);
+    const uint32_t bk = (uint32_t)ch * (uint32_t)sizeof(uint2);
+    mbar_arrive_expect_tx(bar, 2 * bv + bk);
+    bulk_to_smem(sg.A, P.A + base, bv, bar);
+    bulk_to_smem(sg.H, P.H + base, bv, bar);
+    bulk_to_smem(sg.K, P.K + base, bk, bar);
 }
 
 // G2P follows partition_kernel_g2p (kernels.cuh:181-315).  The 3x3 gather is
@@ -526,178 +643,233 @@ __device__ __forceinline__ void patch_add(Patch<Real> &p, const Src<Real> &s, co
 // which equals the reference's sums over the nine nodes (the subtracted v_c
 // cancels because sum_a wx_a (a-1-x) = 0 and sum_b wy_b (b-1-y) = 0) and keeps
 // FP32 roundoff relative to velocity differences.
-template <class Real, class Acc, int BT, int PPT, int CAP>
+//
+// Persistent CTAs walk the chunks c = blockIdx.x, blockIdx.x + gridDim.x, ...
+// The point state of a chunk (A, H, K: 40 B per point in FP32) arrives in
+// shared memory by bulk copy, issued ahead of its use; the G2P gathers read
+// grid velocities through L1; new point state is written to global memory
+// with streaming stores; the P2G terms go through register patches into the
+// shared tile and from there, one atomic per node and channel, to the global
+// accumulators.  Every point of a chunk is read and written by the same
+// thread, so a stage can be refilled as soon as the CTA has passed the
+// barrier after its points.
+template <class Real, class Acc, int BT, int PPT, int CAP, int STAGES>
 __global__ void __launch_bounds__(BT, (sizeof(Real) == 8 ? 1 : ICEMPM_FUSED_MINB))
-k_g2p_p2g(KParams<Real> kp, Pts<Real> P, Grid<Real, Acc> G, DevStatus *st, int n)
+k_g2p_p2g(KParams<Real> kp, Pts<Real> P, Grid<Real, Acc> G, DevStatus *st, int n, int nchunks)
 {
-    __shared__ Acc tile[3][CAP];
-    __shared__ int box[4];
-    init_box(box);
-    const int lane = threadIdx.x & 31;
-    const uint32_t warp = (blockIdx.x * BT + threadIdx.x) >> 5;
+    static_assert(STAGES == 1 || STAGES == 2, "one or two stages");
+    using SM = ChunkSmem<Real, Acc, BT, PPT, CAP, STAGES>;
+    constexpr int CH = SM::CH;
+    constexpr int NW = BT / 32;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    SM &sm = *reinterpret_cast<SM *>(smem_raw);
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
 
-    // tile from the current cells: a point moves at most one cell per step,
-    // so its new 3x3 stencil lies within its old cell +- 2 nodes
-    unsigned xmn = 0x7fffffffu, ymn = 0x7fffffffu, xmx = 0, ymx = 0;
-    bool any = false;
-#pragma unroll
-    for (int j = 0; j < PPT; j++) {
-        const uint32_t i = fused_index<PPT>(warp, lane, j);
-        if (i < (uint32_t)n) {
-            const uint2 key = P.K[i];
-            const int cx = (int)(key.x & 0xffff), cy = (int)(key.x >> 16);
-            if (!(key.y & kDisabled) && cell_in_range(cx, cy, kp.gx, kp.gy)) {
-                xmn = min(xmn, (unsigned)cx); ymn = min(ymn, (unsigned)cy);
-                xmx = max(xmx, (unsigned)cx); ymx = max(ymx, (unsigned)cy);
-                any = true;
-            }
-        }
+    if (tid == 0) {
+        mbar_init(&sm.mbar[0], 1);
+        if (STAGES == 2) mbar_init(&sm.mbar[1], 1);
+        mbar_fence_init();
     }
     __syncthreads();
-    const Tile<Acc, CAP> T = make_tile<Acc, CAP>(tile, box, any, xmn, ymn, xmx, ymx, 2);
-    tile_zero<Acc, CAP, BT>(T);
-    __syncthreads();
+    int c = blockIdx.x;
+    if (tid == 0 && c < nchunks) fetch_chunk(sm.stage[0], P, (uint32_t)c * CH, CH, &sm.mbar[0]);
 
     const int step = st->step;
     const bool recordPQ = kp.update_every > 0 && (step % kp.update_every) == 0;
     const bool store_vc = step == st->vc_step;
     uint32_t err = 0, perr = 0;
     int ndis = 0;
-    Patch<Real> patch;
-    patch.have = false; patch.in_tile = false; patch.cx = patch.cy = 0;
 
-    // the next point's state is loaded one iteration ahead
-    uint32_t inext = fused_index<PPT>(warp, lane, 0);
-    bool vnext = inext < (uint32_t)n;
-    uint2 knext = make_uint2(0u, kDisabled);
-    V4<Real> anext, hnext;
-    if (vnext) { knext = ld_stream(P.K + inext); anext = ld_stream(P.A + inext); hnext = ld_stream(P.H + inext); }
-#pragma unroll 1
-    for (int j = 0; j < PPT; j++) {
-        if (!vnext) break;
-        const uint32_t i = inext;
-        const uint2 key = knext;
-        const V4<Real> A = anext;
-        const V4<Real> Hv = hnext;
-        inext = fused_index<PPT>(warp, lane, j + 1);
-        vnext = j + 1 < PPT && inext < (uint32_t)n;
-        if (vnext) { knext = ld_stream(P.K + inext); anext = ld_stream(P.A + inext); hnext = ld_stream(P.H + inext); }
-        uint32_t util = key.y;
-        if (util & kDisabled) continue;
-        Real x = A.x, y = A.y, Jp = A.z;
-        const Real thick = A.w;
-        M2<Real> H = {Hv.x, Hv.y, Hv.z, Hv.w};
-        int cx = (int)(key.x & 0xffff), cy = (int)(key.x >> 16);
-        Real vx = 0, vy = 0, c00 = 0, c01 = 0, c10 = 0, c11 = 0;
-        if (cell_in_range(cx, cy, kp.gx, kp.gy)) {
-            Real wx[3], wy[3];
-            bspline(x, wx);
-            bspline(y, wy);
-            V2<Real> nv[3][3];
+    for (int it = 0; c < nchunks; it++, c += (int)gridDim.x) {
+        const int s = STAGES == 2 ? (it & 1) : 0;
+        const uint32_t parity = STAGES == 2 ? ((uint32_t)(it >> 1) & 1u) : ((uint32_t)it & 1u);
+        const bool ok = mbar_wait_bounded(&sm.mbar[s], parity);
+        if (__syncthreads_or(!ok)) { err |= kErrBarrierTimeout; break; }
+        if (STAGES == 2 && tid == 0 && c + (int)gridDim.x < nchunks)
+            fetch_chunk(sm.stage[s ^ 1], P, (uint32_t)(c + (int)gridDim.x) * CH, CH, &sm.mbar[s ^ 1]);
+        const typename SM::Stage &sg = sm.stage[s];
+        const uint32_t base = (uint32_t)c * CH;
+        const int wbase = wid * 32 * PPT + lane;
+
+        // box of the chunk's enabled, in-range cells
+        unsigned xmn = 0xffffu, ymn = 0xffffu, xmx = 0, ymx = 0;
+        bool any = false;
 #pragma unroll
-            for (int a = 0; a < 3; a++) {
-                const uint32_t col = (uint32_t)(cx + a - 1) * (uint32_t)kp.gy + (uint32_t)(cy - 1);
-#pragma unroll
-                for (int b = 0; b < 3; b++) nv[a][b] = G.vel[col + b];
-            }
-            const Real gyv[3] = {wy[0] * (Real(-1) - y), wy[1] * (-y), wy[2] * (Real(1) - y)};
-            const Real gxv[3] = {wx[0] * (Real(-1) - x), wx[1] * (-x), wx[2] * (Real(1) - x)};
-            const Real ccx = nv[1][1].x, ccy = nv[1][1].y;
-            Real sx = 0, sy = 0, px = 0, py = 0, qx = 0, qy = 0;
-#pragma unroll
-            for (int a = 0; a < 3; a++) {
-                Real sax = 0, say = 0, tax = 0, tay = 0;
-#pragma unroll
-                for (int b = 0; b < 3; b++) {
-                    const Real dx = nv[a][b].x - ccx, dy = nv[a][b].y - ccy;
-                    sax += wy[b] * dx; say += wy[b] * dy;
-                    tax += gyv[b] * dx; tay += gyv[b] * dy;
+        for (int j = 0; j < PPT; j++) {
+            const int local = wbase + 32 * j;
+            if (base + (uint32_t)local < (uint32_t)n) {
+                const uint2 key = sg.K[local];
+                const int cx = (int)(key.x & 0xffff), cy = (int)(key.x >> 16);
+                if (!(key.y & kDisabled) && cell_in_range(cx, cy, kp.gx, kp.gy)) {
+                    xmn = min(xmn, (unsigned)cx); ymn = min(ymn, (unsigned)cy);
+                    xmx = max(xmx, (unsigned)cx); ymx = max(ymx, (unsigned)cy);
+                    any = true;
                 }
-                sx += wx[a] * sax; sy += wx[a] * say;     // v_p - v_c
-                px += gxv[a] * sax; py += gxv[a] * say;   // x-derivative part
-                qx += wx[a] * tax; qy += wx[a] * tay;     // y-derivative part
             }
-            vx = ccx + sx; vy = ccy + sy;
-            c00 = kp.four_h_inv * px; c10 = kp.four_h_inv * py;
-            c01 = kp.four_h_inv * qx; c11 = kp.four_h_inv * qy;
         }
-        x += vx * kp.dt_h_inv;
-        y += vy * kp.dt_h_inv;
-        if (isnan(vx + vy)) err |= kErrVelNan;
-        if (isnan(x + y)) err |= kErrPosNan;
-        if (isnan((c00 + c10) + (c01 + c11))) err |= kErrBpNan;
-        bool moved = false;
-        if (x > Real(0.5)) { x -= Real(1); cx++; moved = true; }
-        else if (x < Real(-0.5)) { x += Real(1); cx--; moved = true; }
-        if (y > Real(0.5)) { y -= Real(1); cy++; moved = true; }
-        else if (y < Real(-0.5)) { y += Real(1); cy--; moved = true; }
-        if (moved && (cx <= 1 || cx >= kp.gx - 2 || cy <= 1 || cy >= kp.gy - 2)) {
-            util |= kDisabled;
-            ndis++;
-        }
-        if (x > Real(0.5) || x < Real(-0.5) || y > Real(0.5) || y < Real(-0.5)) err |= kErrJump;
-
-        // Fe <- (I + dt C) Fe, i.e. H <- H + D + D H with D = dt C
         {
-            const Real d00 = kp.dt * c00, d01 = kp.dt * c01, d10 = kp.dt * c10, d11 = kp.dt * c11;
-            const M2<Real> h = H;
-            H.a00 = h.a00 + d00 + (d00 * h.a00 + d01 * h.a10);
-            H.a01 = h.a01 + d01 + (d00 * h.a01 + d01 * h.a11);
-            H.a10 = h.a10 + d10 + (d10 * h.a00 + d11 * h.a10);
-            H.a11 = h.a11 + d11 + (d10 * h.a01 + d11 * h.a11);
-        }
-        if (isnan((H.a00 + H.a10) + (H.a01 + H.a11))) err |= kErrFeNan;
-        Kin<Real> k = kinematics(H);
-        Real p_tr, q_tr;
-        pq(k, Real(kp.mat.mu), Real(kp.mat.kappa), p_tr, q_tr);
-        if (!(util & kCrushed)) util = failure_check(kp.mat, util, p_tr, q_tr);
-        if (util & kCrushed) {
-            const SvdH<Real> sv = svd_h(H);
-            wolper_dp(kp.mat, thick, p_tr, q_tr, k, sv, H, Jp);
-            if (isnan((H.a00 + H.a10) + (H.a01 + H.a11))) err |= kErrFeNan;
-            k = kinematics(H);
-        }
-
-        V4<Real> Ao; Ao.x = x; Ao.y = y; Ao.z = Jp; Ao.w = thick;
-        st_stream(P.A + i, Ao);
-        V4<Real> Ho; Ho.x = H.a00; Ho.y = H.a01; Ho.z = H.a10; Ho.w = H.a11;
-        st_stream(P.H + i, Ho);
-        if (store_vc || (util & kDisabled)) {   // a point disabled now keeps this step's V and C
-            V2<Real> Vo; Vo.x = vx; Vo.y = vy;
-            st_stream(P.V + i, Vo);
-            V4<Real> Co; Co.x = c00; Co.y = c01; Co.z = c10; Co.w = c11;
-            st_stream(P.C + i, Co);
-        }
-        const uint32_t cell = ((uint32_t)cy << 16) | (uint32_t)cx;   // as kernels.cuh:305
-        if (moved || util != key.y) {
-            uint2 ko; ko.x = moved ? cell : key.x; ko.y = util;
-            st_stream(P.K + i, ko);
-        }
-        if (recordPQ) { V2<Real> pqv; pqv.x = p_tr; pqv.y = q_tr; st_stream(P.PQ + i, pqv); }
-
-        if (!(util & kDisabled)) {
-            if (cell_in_range(cx, cy, kp.gx, kp.gy)) {
-                Src<Real> s;
-                s.cx = cx; s.cy = cy;
-                make_src<Real, Acc>(kp, G.frc, s, x, y, Jp, thick, k, vx, vy, c00, c01, c10, c11, perr);
-                // NaN reaches these sums from any NaN term (the scatter's NaN checks)
-                const Real sw = (s.wx[0] + s.wx[1] + s.wx[2]) + (s.wy[0] + s.wy[1] + s.wy[2]);
-                if (isnan(sw + s.mp)) perr |= kErrP2gNanMass;
-                if (isnan(sw + ((s.ax + s.ay) + (s.s00 + s.s01) + (s.s10 + s.s11)))) perr |= kErrP2gNanVel;
-                patch_add<Real, Acc, CAP>(patch, s, T, G.acc, kp.gy);
-            } else {
-                perr |= kErrLeftArea;
+            const unsigned FULL = 0xffffffffu;
+            xmn = __reduce_min_sync(FULL, xmn); ymn = __reduce_min_sync(FULL, ymn);
+            xmx = __reduce_max_sync(FULL, xmx); ymx = __reduce_max_sync(FULL, ymx);
+            const unsigned wany = __reduce_or_sync(FULL, any ? 1u : 0u);
+            if (lane == 0) {
+                sm.red[wid][0] = (int)xmn; sm.red[wid][1] = (int)ymn;
+                sm.red[wid][2] = (int)xmx; sm.red[wid][3] = (int)ymx; sm.red[wid][4] = (int)wany;
             }
         }
+        __syncthreads();
+        int bx0 = 0xffff, by0 = 0xffff, bx1 = 0, by1 = 0, bany = 0;
+#pragma unroll
+        for (int w = 0; w < NW; w++) {
+            bx0 = min(bx0, sm.red[w][0]); by0 = min(by0, sm.red[w][1]);
+            bx1 = max(bx1, sm.red[w][2]); by1 = max(by1, sm.red[w][3]); bany |= sm.red[w][4];
+        }
+        // scatter tile: cells +-2 (a point moves at most one cell per step)
+        Tile<Acc, CAP> T;
+        T.t = sm.tile;
+        T.x0 = bx0 - 2; T.y0 = by0 - 2;
+        T.tw = bx1 - bx0 + 5; T.th = by1 - by0 + 5;
+        // 64-bit products: a box spanning the whole grid must not wrap into range
+        T.on = bany && (long long)T.tw * (long long)T.th <= (long long)CAP;
+        if (!T.on) { T.tw = 0; T.th = 0; }
+        T.th_rcp = rcp32(T.th);
+        tile_zero<Acc, CAP, BT>(T);
+        __syncthreads();
+
+        Patch<Real> patch;
+        patch.have = false; patch.in_tile = false; patch.cx = patch.cy = 0;
+#pragma unroll 1
+        for (int j = 0; j < PPT; j++) {
+            const int local = wbase + 32 * j;
+            const uint32_t i = base + (uint32_t)local;
+            if (i >= (uint32_t)n) break;
+            const uint2 key = sg.K[local];
+            uint32_t util = key.y;
+            if (util & kDisabled) continue;
+            const V4<Real> A = sg.A[local];
+            const V4<Real> Hv = sg.H[local];
+            Real x = A.x, y = A.y, Jp = A.z;
+            const Real thick = A.w;
+            M2<Real> H = {Hv.x, Hv.y, Hv.z, Hv.w};
+            int cx = (int)(key.x & 0xffff), cy = (int)(key.x >> 16);
+            // forcing entry of the current cell, loaded early (points rarely change cell)
+            V4<Real> frc{};
+            if (kp.ext && cell_in_range(cx, cy, kp.gx, kp.gy)) frc = G.frc[(uint32_t)cx * (uint32_t)kp.gy + (uint32_t)cy];
+            Real vx = 0, vy = 0, c00 = 0, c01 = 0, c10 = 0, c11 = 0;
+            if (cell_in_range(cx, cy, kp.gx, kp.gy)) {
+                Real wx[3], wy[3];
+                bspline(x, wx);
+                bspline(y, wy);
+                V2<Real> nv[3][3];
+#pragma unroll
+                for (int a = 0; a < 3; a++) {
+                    const uint32_t col = (uint32_t)(cx + a - 1) * (uint32_t)kp.gy + (uint32_t)(cy - 1);
+#pragma unroll
+                    for (int b = 0; b < 3; b++) nv[a][b] = G.vel[col + b];
+                }
+                const Real gyv[3] = {wy[0] * (Real(-1) - y), wy[1] * (-y), wy[2] * (Real(1) - y)};
+                const Real gxv[3] = {wx[0] * (Real(-1) - x), wx[1] * (-x), wx[2] * (Real(1) - x)};
+                const Real ccx = nv[1][1].x, ccy = nv[1][1].y;
+                Real sx = 0, sy = 0, px = 0, py = 0, qx = 0, qy = 0;
+#pragma unroll
+                for (int a = 0; a < 3; a++) {
+                    Real sax = 0, say = 0, tax = 0, tay = 0;
+#pragma unroll
+                    for (int b = 0; b < 3; b++) {
+                        const Real dx = nv[a][b].x - ccx, dy = nv[a][b].y - ccy;
+                        sax += wy[b] * dx; say += wy[b] * dy;
+                        tax += gyv[b] * dx; tay += gyv[b] * dy;
+                    }
+                    sx += wx[a] * sax; sy += wx[a] * say;     // v_p - v_c
+                    px += gxv[a] * sax; py += gxv[a] * say;   // x-derivative part
+                    qx += wx[a] * tax; qy += wx[a] * tay;     // y-derivative part
+                }
+                vx = ccx + sx; vy = ccy + sy;
+                c00 = kp.four_h_inv * px; c10 = kp.four_h_inv * py;
+                c01 = kp.four_h_inv * qx; c11 = kp.four_h_inv * qy;
+            }
+            x += vx * kp.dt_h_inv;
+            y += vy * kp.dt_h_inv;
+            if (isnan(vx + vy)) err |= kErrVelNan;
+            if (isnan(x + y)) err |= kErrPosNan;
+            if (isnan((c00 + c10) + (c01 + c11))) err |= kErrBpNan;
+            bool moved = false;
+            if (x > Real(0.5)) { x -= Real(1); cx++; moved = true; }
+            else if (x < Real(-0.5)) { x += Real(1); cx--; moved = true; }
+            if (y > Real(0.5)) { y -= Real(1); cy++; moved = true; }
+            else if (y < Real(-0.5)) { y += Real(1); cy--; moved = true; }
+            if (moved && (cx <= 1 || cx >= kp.gx - 2 || cy <= 1 || cy >= kp.gy - 2)) {
+                util |= kDisabled;
+                ndis++;
+            }
+            if (x > Real(0.5) || x < Real(-0.5) || y > Real(0.5) || y < Real(-0.5)) err |= kErrJump;
+
+            // Fe <- (I + dt C) Fe, i.e. H <- H + D + D H with D = dt C
+            {
+                const Real d00 = kp.dt * c00, d01 = kp.dt * c01, d10 = kp.dt * c10, d11 = kp.dt * c11;
+                const M2<Real> h = H;
+                H.a00 = h.a00 + d00 + (d00 * h.a00 + d01 * h.a10);
+                H.a01 = h.a01 + d01 + (d00 * h.a01 + d01 * h.a11);
+                H.a10 = h.a10 + d10 + (d10 * h.a00 + d11 * h.a10);
+                H.a11 = h.a11 + d11 + (d10 * h.a01 + d11 * h.a11);
+            }
+            if (isnan((H.a00 + H.a10) + (H.a01 + H.a11))) err |= kErrFeNan;
+            Kin<Real> k = kinematics(H);
+            Real p_tr, q_tr;
+            pq(k, kp.mat.mu, kp.mat.kappa, p_tr, q_tr);
+            if (!(util & kCrushed)) util = failure_check(kp.mat, util, p_tr, q_tr);
+            if (util & kCrushed) {
+                const SvdH<Real> sv = svd_h(H);
+                wolper_dp(kp.mat, thick, p_tr, q_tr, k, sv, H, Jp);
+                if (isnan((H.a00 + H.a10) + (H.a01 + H.a11))) err |= kErrFeNan;
+                k = kinematics(H);
+            }
+
+            V4<Real> Ao; Ao.x = x; Ao.y = y; Ao.z = Jp; Ao.w = thick;
+            st_stream(P.A + i, Ao);
+            V4<Real> Ho; Ho.x = H.a00; Ho.y = H.a01; Ho.z = H.a10; Ho.w = H.a11;
+            st_stream(P.H + i, Ho);
+            if (store_vc || (util & kDisabled)) {   // a point disabled now keeps this step's V and C
+                V2<Real> Vo; Vo.x = vx; Vo.y = vy;
+                st_stream(P.V + i, Vo);
+                V4<Real> Co; Co.x = c00; Co.y = c01; Co.z = c10; Co.w = c11;
+                st_stream(P.C + i, Co);
+            }
+            const uint32_t cell = ((uint32_t)cy << 16) | (uint32_t)cx;   // as kernels.cuh:305
+            if (moved || util != key.y) {
+                uint2 ko; ko.x = moved ? cell : key.x; ko.y = util;
+                st_stream(P.K + i, ko);
+            }
+            if (recordPQ) { V2<Real> pqv; pqv.x = p_tr; pqv.y = q_tr; st_stream(P.PQ + i, pqv); }
+
+            if (!(util & kDisabled)) {
+                if (cell_in_range(cx, cy, kp.gx, kp.gy)) {
+                    Src<Real> src;
+                    src.cx = cx; src.cy = cy;
+                    if (kp.ext && moved) frc = G.frc[(uint32_t)cx * (uint32_t)kp.gy + (uint32_t)cy];
+                    make_src<Real, Acc>(kp, frc, src, x, y, Jp, thick, k, vx, vy, c00, c01, c10, c11, perr);
+                    // NaN reaches these sums from any NaN term (the scatter's NaN checks)
+                    const Real sw = (src.wx[0] + src.wx[1] + src.wx[2]) + (src.wy[0] + src.wy[1] + src.wy[2]);
+                    if (isnan(sw + src.mp)) perr |= kErrP2gNanMass;
+                    if (isnan(sw + ((src.ax + src.ay) + (src.s00 + src.s01) + (src.s10 + src.s11)))) perr |= kErrP2gNanVel;
+                    patch_add<Real, Acc, CAP>(patch, src, T, G.acc, kp.gy);
+                } else {
+                    perr |= kErrLeftArea;
+                }
+            }
+        }
+        if (patch.have) patch_flush<Real, Acc, CAP>(patch, T, G.acc, kp.gy);
+        __syncthreads();
+        // one stage: its points are all read now, fetch the next chunk into it
+        if (STAGES == 1 && tid == 0 && c + (int)gridDim.x < nchunks)
+            fetch_chunk(sm.stage[0], P, (uint32_t)(c + (int)gridDim.x) * CH, CH, &sm.mbar[0]);
+        tile_flush<Acc, CAP, BT>(T, G.acc, kp.gx, kp.gy);
     }
-    if (patch.have) patch_flush<Real, Acc, CAP>(patch, T, G.acc, kp.gy);
-    __syncthreads();
-    tile_flush<Acc, CAP, BT>(T, G.acc, kp.gx, kp.gy);
     warp_flush_status(st, err, perr, ndis);
 
     // the last CTA to finish advances the device step counter (no waiting)
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (tid == 0) {
         __threadfence();
         const unsigned t = atomicAdd(&st->done, 1u);
         if (t == gridDim.x - 1) {

@@ -24,11 +24,17 @@ static inline double pow2_floor(double x) { return std::ldexp(1.0, (int)std::flo
 
 template <class Real, class Acc>
 class EngineT final : public Engine {
-    static constexpr int BT = 128;       // threads per CTA of the fused kernel
-    static constexpr int PPT = ICEMPM_FUSED_PPT;   // points per thread of the fused kernel
-    static constexpr int CAP = 1024;     // nodes in the shared scatter tile
+    // fused kernel: threads per CTA and points per thread (a chunk of BT*PPT
+    // points per CTA iteration; FP64 state halves the chunk to fit two stages)
+    static constexpr int BT = sizeof(Real) == 8 ? 128 : ICEMPM_FUSED_BT;
+    static constexpr int PPT = sizeof(Real) == 8 ? 2 : ICEMPM_FUSED_PPT;
+    static constexpr int CH = BT * PPT;
+    static constexpr int CAP = ICEMPM_FUSED_CAP;     // nodes in the shared scatter tile
     static constexpr int BT_P2G = 256;   // threads per CTA of the priming scatter
     static constexpr int GRAPH_STEPS = 32;
+    static constexpr size_t PAD = 2048;  // point arrays are padded to whole chunks
+    static constexpr int STAGES = ICEMPM_FUSED_STAGES;
+    using FusedSmem = ChunkSmem<Real, Acc, BT, PPT, CAP, STAGES>;
 
 public:
     EngineT() = default;
@@ -51,7 +57,7 @@ public:
         ICEMPM_CUDA(cudaEventCreate(&evs_[1]));
         ICEMPM_CUDA(cudaEventCreate(&evs_[2]));
         // points, two parities for the sort gather
-        const size_t nc = ((size_t)cap_ + 255) / 256 * 256;
+        const size_t nc = ((size_t)cap_ + PAD - 1) / PAD * PAD;   // the bulk copies read whole chunks
         const size_t per = nc * (3 * sizeof(V4<Real>) + 2 * sizeof(V2<Real>) + sizeof(uint2) + 2 * sizeof(uint32_t) + sizeof(double));
         ICEMPM_CUDA(cudaMalloc(&pts_mem_, 2 * per));
         for (int par = 0; par < 2; par++) {
@@ -100,6 +106,14 @@ public:
         // 4 points per cell: 8 columns of BT*PPT/32 cells
         tile_.tx = 8; tile_.ty = BT * PPT / 32;
         tile_.ntiles_y = (gy_ + tile_.ty - 1) / tile_.ty;
+        // persistent grid of the fused kernel: as many CTAs as fit on the device
+        auto kern = k_g2p_p2g<Real, Acc, BT, PPT, CAP, STAGES>;
+        ICEMPM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(FusedSmem)));
+        int per_sm = 0, sms = 0;
+        ICEMPM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, BT, sizeof(FusedSmem)));
+        ICEMPM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, o.device));
+        if (per_sm < 1) return fail(ICEMPM_E_UNSUPPORTED, "fused kernel does not fit on one SM");
+        fused_ctas_ = per_sm * sms;
         return set_params(p, 1.0);
     }
 
@@ -130,7 +144,7 @@ public:
         k.lim_p = (float)(std::ldexp(1.0, 56) / k.scale_p);
         k.ext_impulse = Real(p.InitialTimeStep * p.ParticleVolume);
         k.rho_w_cd = Real(opts_.water_density * opts_.water_drag_coeff);
-        Material &m = k.mat;
+        Material m;
         m.mu = p.mu; m.kappa = p.kappa; m.DP_threshold_p = p.DP_threshold_p;
         m.pmax = p.IceCompressiveStrength; m.pmin = -p.IceTensileStrength;
         m.qmax = p.IceShearStrength; m.pmin2 = -p.IceTensileStrength2;
@@ -138,6 +152,7 @@ public:
         m.M_sq = (4. * m.qmax * m.qmax * (1. + 2. * m.beta)) / ((m.pmax - m.pmin) * (m.pmax - m.pmin));
         m.tan_phi = std::tan(p.DP_phi * ICEMPM_PI / 180);
         m.ridge_coeff_g_rho = p.RidgeFormationCoeff * ICEMPM_GRAVITY * p.IceDensity;
+        k.mat = mat_of<Real>(m);
         primed_ = false;
         invalidate_graphs();
         return 0;
@@ -256,9 +271,10 @@ public:
 
     void launch_fused()
     {
-        const size_t warps = ((size_t)n_ + 32 * PPT - 1) / (32 * PPT);
-        const unsigned nb = (unsigned)((warps + BT / 32 - 1) / (BT / 32));
-        k_g2p_p2g<Real, Acc, BT, PPT, CAP><<<nb, BT, 0, stream_>>>(kp_, pts_[par_], grid(), st_, (int)n_);
+        const int nchunks = (int)(((size_t)n_ + CH - 1) / CH);
+        const unsigned nb = (unsigned)(ICEMPM_FUSED_PERSIST ? std::min(nchunks, fused_ctas_) : nchunks);
+        k_g2p_p2g<Real, Acc, BT, PPT, CAP, STAGES>
+            <<<nb, BT, sizeof(FusedSmem), stream_>>>(kp_, pts_[par_], grid(), st_, (int)n_, nchunks);
         launches_++;
     }
     int prime()
@@ -530,6 +546,7 @@ private:
     TileKey tile_{8, 8, 1};
     KParams<Real> kp_{};
     bool primed_ = false, timed_ = false;
+    int fused_ctas_ = 1;
     int steps_since_sort_ = 0;
     float last_sort_ms_ = 0;
     cudaGraphExec_t graph_exec_ = nullptr;

@@ -4,7 +4,7 @@
 #include <cstdint>
 #include <string>
 #include <cuda_runtime.h>
-#include "../../include/icempm.h"
+#include "icempm.h"
 
 namespace icempm {
 

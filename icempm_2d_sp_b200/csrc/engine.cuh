@@ -28,7 +28,7 @@
 //   PQ  {P, Q}                     written on record steps only
 //   slot, pid, thick64             host slot, point id row, f64 thickness
 // Grid layout (node = y + x*GridY, the reference order):
-//   acc {mass, px, py, -}          accumulators (int64 fixed point, f32 or f64)
+//   acc.m, acc.px, acc.py          accumulators, one array each (int64 fixed point, f32 or f64)
 //   vel {vx, vy}                   grid velocity after the update
 //   status (u8), cur {vx, vy}, force {fx, fy} (f64, boundary reaction)
 #pragma once
@@ -72,7 +72,9 @@ namespace icempm {
 
 template <class T> struct alignas(16) V4 { T x, y, z, w; };
 template <class T> struct alignas(2 * sizeof(T) > 16 ? 16 : 2 * sizeof(T)) V2 { T x, y; };
-template <class A> struct alignas(16) Acc4 { A m, px, py, pad; };
+// Grid accumulators, one array per channel (node-major), so that a warp's
+// atomics and the grid update's loads touch contiguous words.
+template <class A> struct AccGrid { A *m, *px, *py; };
 
 // Point arrays are read once and written once per step: load and store them
 // with the streaming cache policy so they do not evict the grid velocities
@@ -130,7 +132,7 @@ template <class Real> struct Pts {
 };
 
 template <class Real, class Acc> struct Grid {
-    Acc4<Acc> *acc;
+    AccGrid<Acc> acc;
     V2<Real> *vel;
     V2<Real> *cur;
     const V4<Real> *frc;   // extended forcing per node: {current vx, vy, wind stress x, y}
@@ -273,7 +275,7 @@ template <class Acc, int CAP> struct Tile {
 __device__ __forceinline__ unsigned rcp32(int d) { return d > 0 ? 0xffffffffu / (unsigned)d + 1u : 0u; }
 
 template <class Real, class Acc, int CAP>
-__device__ __forceinline__ void node_add(const Tile<Acc, CAP> &T, bool in_tile, Acc4<Acc> *__restrict__ gacc,
+__device__ __forceinline__ void node_add(const Tile<Acc, CAP> &T, bool in_tile, const AccGrid<Acc> &gacc,
                                          int gy, int X, int Y, Real m, Real px, Real py)
 {
     const Acc am = AccOps<Acc>::cvt(m), ax = AccOps<Acc>::cvt(px), ay = AccOps<Acc>::cvt(py);
@@ -284,9 +286,9 @@ __device__ __forceinline__ void node_add(const Tile<Acc, CAP> &T, bool in_tile, 
         AccOps<Acc>::add_shared(&T.t[2][li], ay);
     } else {
         const uint32_t node = (uint32_t)X * (uint32_t)gy + (uint32_t)Y;
-        AccOps<Acc>::add_global(&gacc[node].m, am);
-        AccOps<Acc>::add_global(&gacc[node].px, ax);
-        AccOps<Acc>::add_global(&gacc[node].py, ay);
+        AccOps<Acc>::add_global(gacc.m + node, am);
+        AccOps<Acc>::add_global(gacc.px + node, ax);
+        AccOps<Acc>::add_global(gacc.py + node, ay);
     }
 }
 
@@ -302,7 +304,7 @@ __device__ __forceinline__ void tile_zero(const Tile<Acc, CAP> &T)
 
 // One global atomic per non-zero tile entry and channel (all threads of the CTA).
 template <class Acc, int CAP, int BT>
-__device__ __forceinline__ void tile_flush(const Tile<Acc, CAP> &T, Acc4<Acc> *__restrict__ gacc, int gx, int gy)
+__device__ __forceinline__ void tile_flush(const Tile<Acc, CAP> &T, const AccGrid<Acc> &gacc, int gx, int gy)
 {
     const int nt = T.tw * T.th;
     for (int k = threadIdx.x; k < nt; k += BT) {
@@ -311,9 +313,9 @@ __device__ __forceinline__ void tile_flush(const Tile<Acc, CAP> &T, Acc4<Acc> *_
         const Acc m = T.t[0][k], px = T.t[1][k], py = T.t[2][k];
         if ((m != Acc(0) || px != Acc(0) || py != Acc(0)) && X >= 0 && X < gx && Y >= 0 && Y < gy) {
             const uint32_t node = (uint32_t)X * (uint32_t)gy + (uint32_t)Y;
-            if (m != Acc(0)) AccOps<Acc>::add_global(&gacc[node].m, m);
-            if (px != Acc(0)) AccOps<Acc>::add_global(&gacc[node].px, px);
-            if (py != Acc(0)) AccOps<Acc>::add_global(&gacc[node].py, py);
+            if (m != Acc(0)) AccOps<Acc>::add_global(gacc.m + node, m);
+            if (px != Acc(0)) AccOps<Acc>::add_global(gacc.px + node, px);
+            if (py != Acc(0)) AccOps<Acc>::add_global(gacc.py + node, py);
         }
     }
 }
@@ -428,16 +430,14 @@ __global__ void __launch_bounds__(256) k_grid_update(KParams<Real> kp, Grid<Real
         if (pe) { atomicOr(&st->err, pe); st->err_pending = 0; }
     }
     if (idx >= nnodes) return;
-    const Acc4<Acc> r = G.acc[idx];
+    struct { Acc m, px, py; } r = {G.acc.m[idx], G.acc.px[idx], G.acc.py[idx]};
     V2<Real> out;
     out.x = Real(0); out.y = Real(0);
     if (r.m == Acc(0) && r.px == Acc(0) && r.py == Acc(0)) {
         G.vel[idx] = out;
         return;
     }
-    Acc4<Acc> z;
-    z.m = z.px = z.py = z.pad = Acc(0);
-    G.acc[idx] = z;
+    G.acc.m[idx] = Acc(0); G.acc.px[idx] = Acc(0); G.acc.py[idx] = Acc(0);
     const Real mass = AccOps<Acc>::template to<Real>(r.m, kp.inv_scale_m);
     uint32_t err = 0;
     if (mass != Real(0)) {
@@ -539,7 +539,7 @@ template <class Real> struct Patch {
 };
 
 template <class Real, class Acc, int CAP>
-__device__ __forceinline__ void patch_flush(Patch<Real> &p, const Tile<Acc, CAP> &T, Acc4<Acc> *gacc, int gy)
+__device__ __forceinline__ void patch_flush(Patch<Real> &p, const Tile<Acc, CAP> &T, const AccGrid<Acc> &gacc, int gy)
 {
 #pragma unroll
     for (int a = 0; a < 3; a++)
@@ -547,6 +547,52 @@ __device__ __forceinline__ void patch_flush(Patch<Real> &p, const Tile<Acc, CAP>
         for (int b = 0; b < 3; b++)
             node_add<Real, Acc, CAP>(T, p.in_tile, gacc, gy, p.cx + a - 1, p.cy + b - 1, p.m[a][b], p.px[a][b], p.py[a][b]);
     p.have = false;
+}
+
+// Writes out a tile patch with its lowest (b = 0) and highest (b = 2) node
+// rows only where asked: a row another lane has taken over is skipped.
+template <class Real, class Acc, int CAP>
+__device__ __forceinline__ void patch_flush_rows(Patch<Real> &p, const Tile<Acc, CAP> &T, const AccGrid<Acc> &gacc, int gy,
+                                                 bool low, bool high)
+{
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        if (low) node_add<Real, Acc, CAP>(T, p.in_tile, gacc, gy, p.cx + a - 1, p.cy - 1, p.m[a][0], p.px[a][0], p.py[a][0]);
+        node_add<Real, Acc, CAP>(T, p.in_tile, gacc, gy, p.cx + a - 1, p.cy, p.m[a][1], p.px[a][1], p.py[a][1]);
+        if (high) node_add<Real, Acc, CAP>(T, p.in_tile, gacc, gy, p.cx + a - 1, p.cy + 1, p.m[a][2], p.px[a][2], p.py[a][2]);
+    }
+    p.have = false;
+}
+
+// End of a chunk: lanes whose tile patches sit on vertically adjacent cells
+// of one column (lane l+1 one cell above lane l, the usual case in the
+// interleaved cell order) overlap in two node rows.  Each lane adds the
+// upper neighbour's lowest row and the lower neighbour's highest row into
+// its centre row with warp shuffles (a fixed order of float adds, so the
+// fixed-point sums stay deterministic), and only rows no neighbour took are
+// written out: in the usual case 9 of the 27 node-channel adds remain.
+// All 32 lanes of the warp must call it.
+template <class Real, class Acc, int CAP>
+__device__ __forceinline__ void patch_merge_flush(Patch<Real> &p, const Tile<Acc, CAP> &T, const AccGrid<Acc> &gacc, int gy,
+                                                  int lane)
+{
+    const unsigned FULL = 0xffffffffu;
+    const bool mine = p.have && p.in_tile;
+    const uint32_t key = mine ? (((uint32_t)p.cx << 16) | (uint32_t)p.cy) : 0xffffffffu;
+    const uint32_t key_up = __shfl_down_sync(FULL, key, 1);     // lane l+1
+    const uint32_t key_dn = __shfl_up_sync(FULL, key, 1);       // lane l-1
+    const bool above = mine && lane < 31 && key_up == key + 1u;
+    const bool below = mine && lane > 0 && key_dn == key - 1u;
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        const Real um = __shfl_down_sync(FULL, p.m[a][0], 1), ux = __shfl_down_sync(FULL, p.px[a][0], 1),
+                   uy = __shfl_down_sync(FULL, p.py[a][0], 1);
+        const Real dm = __shfl_up_sync(FULL, p.m[a][2], 1), dx = __shfl_up_sync(FULL, p.px[a][2], 1),
+                   dy = __shfl_up_sync(FULL, p.py[a][2], 1);
+        if (above) { p.m[a][1] += um; p.px[a][1] += ux; p.py[a][1] += uy; }
+        if (below) { p.m[a][1] += dm; p.px[a][1] += dx; p.py[a][1] += dy; }
+    }
+    if (p.have) patch_flush_rows<Real, Acc, CAP>(p, T, gacc, gy, !below, !above);
 }
 
 // The node terms of src_terms, summed separably: with
@@ -576,7 +622,7 @@ template <class Real> __device__ __forceinline__ void patch_accumulate(Patch<Rea
 
 template <class Real, class Acc, int CAP>
 __device__ __forceinline__ void patch_add(Patch<Real> &p, const Src<Real> &s, const Tile<Acc, CAP> &T,
-                                          Acc4<Acc> *gacc, int gy)
+                                          const AccGrid<Acc> &gacc, int gy)
 {
     if (p.have) {
         const bool same = s.cx == p.cx && s.cy == p.cy;
@@ -858,7 +904,7 @@ k_g2p_p2g(KParams<Real> kp, Pts<Real> P, Grid<Real, Acc> G, DevStatus *st, int n
                 }
             }
         }
-        if (patch.have) patch_flush<Real, Acc, CAP>(patch, T, G.acc, kp.gy);
+        patch_merge_flush<Real, Acc, CAP>(patch, T, G.acc, kp.gy, lane);
         __syncthreads();
         // one stage: its points are all read now, fetch the next chunk into it
         if (STAGES == 1 && tid == 0 && c + (int)gridDim.x < nchunks)

@@ -75,14 +75,14 @@ public:
             P.pid = (uint32_t *)take(nc * sizeof(uint32_t));
         }
         // grid
-        ICEMPM_CUDA(cudaMalloc(&acc_, G_ * sizeof(Acc4<Acc>)));
+        ICEMPM_CUDA(cudaMalloc(&acc_, 3 * G_ * sizeof(Acc)));
         ICEMPM_CUDA(cudaMalloc(&vel_, G_ * sizeof(V2<Real>)));
         ICEMPM_CUDA(cudaMalloc(&cur_, G_ * sizeof(V2<Real>)));
         ICEMPM_CUDA(cudaMalloc(&frc_, G_ * sizeof(V4<Real>)));
         ICEMPM_CUDA(cudaMalloc(&status_, G_));
         ICEMPM_CUDA(cudaMalloc(&force_, G_ * sizeof(double2)));
         ICEMPM_CUDA(cudaMalloc(&st_, sizeof(DevStatus)));
-        ICEMPM_CUDA(cudaMemsetAsync(acc_, 0, G_ * sizeof(Acc4<Acc>), stream_));
+        ICEMPM_CUDA(cudaMemsetAsync(acc_, 0, 3 * G_ * sizeof(Acc), stream_));
         ICEMPM_CUDA(cudaMemsetAsync(vel_, 0, G_ * sizeof(V2<Real>), stream_));
         ICEMPM_CUDA(cudaMemsetAsync(force_, 0, G_ * sizeof(double2), stream_));
         ICEMPM_CUDA(cudaMemsetAsync(st_, 0, sizeof(DevStatus), stream_));
@@ -279,7 +279,7 @@ public:
     }
     int prime()
     {
-        ICEMPM_CUDA(cudaMemsetAsync(acc_, 0, G_ * sizeof(Acc4<Acc>), stream_));
+        ICEMPM_CUDA(cudaMemsetAsync(acc_, 0, 3 * G_ * sizeof(Acc), stream_));
         ICEMPM_CUDA(cudaMemsetAsync(&st_->err_pending, 0, sizeof(uint32_t), stream_));
         if (n_ > 0) {
             const unsigned nb = (n_ + BT_P2G - 1) / BT_P2G;
@@ -500,7 +500,7 @@ private:
     Grid<Real, Acc> grid() const
     {
         Grid<Real, Acc> g;
-        g.acc = acc_; g.vel = vel_; g.cur = cur_; g.frc = frc_; g.status = status_; g.force = force_;
+        g.acc.m = acc_; g.acc.px = acc_ + G_; g.acc.py = acc_ + 2 * G_; g.vel = vel_; g.cur = cur_; g.frc = frc_; g.status = status_; g.force = force_;
         return g;
     }
     void invalidate_graphs()
@@ -532,7 +532,7 @@ private:
     void *pts_mem_ = nullptr;
     Pts<Real> pts_[2]{};
     int par_ = 0;
-    Acc4<Acc> *acc_ = nullptr;
+    Acc *acc_ = nullptr;   // mass, x- and y-momentum arrays of G_ each
     V2<Real> *vel_ = nullptr, *cur_ = nullptr;
     V4<Real> *frc_ = nullptr;
     uint8_t *status_ = nullptr;

@@ -155,6 +155,21 @@ template <class Real> struct KParams {
     MatT<Real> mat;
 };
 
+// Fire-and-forget reductions into global memory (red.global: no value comes
+// back, so the issuing thread does not wait for the L2).
+__device__ __forceinline__ void red_global_add(long long *a, long long v)
+{
+    asm volatile("red.relaxed.gpu.global.add.u64 [%0], %1;" ::"l"(a), "l"(v) : "memory");
+}
+__device__ __forceinline__ void red_global_add(float *a, float v)
+{
+    asm volatile("red.relaxed.gpu.global.add.f32 [%0], %1;" ::"l"(a), "f"(v) : "memory");
+}
+__device__ __forceinline__ void red_global_add(double *a, double v)
+{
+    asm volatile("red.relaxed.gpu.global.add.f64 [%0], %1;" ::"l"(a), "d"(v) : "memory");
+}
+
 // ---- accumulator conversions -------------------------------------------
 // Scatter values arrive already multiplied by the scale (sources are scaled
 // once per point); `cvt` rounds them to the accumulator type.
@@ -168,23 +183,21 @@ template <> struct AccOps<long long> {
     static __device__ __forceinline__ void add_shared(long long *a, long long v) {
         atomicAdd(reinterpret_cast<unsigned long long *>(a), (unsigned long long)v);
     }
-    static __device__ __forceinline__ void add_global(long long *a, long long v) {
-        atomicAdd(reinterpret_cast<unsigned long long *>(a), (unsigned long long)v);
-    }
+    static __device__ __forceinline__ void add_global(long long *a, long long v) { red_global_add(a, v); }
 };
 template <> struct AccOps<float> {
     static constexpr bool fixed = false;
     template <class R> static __device__ __forceinline__ float cvt(R v) { return float(v); }
     template <class Real> static __device__ __forceinline__ Real to(float v, double) { return Real(v); }
     static __device__ __forceinline__ void add_shared(float *a, float v) { atomicAdd(a, v); }
-    static __device__ __forceinline__ void add_global(float *a, float v) { atomicAdd(a, v); }
+    static __device__ __forceinline__ void add_global(float *a, float v) { red_global_add(a, v); }
 };
 template <> struct AccOps<double> {
     static constexpr bool fixed = false;
     template <class R> static __device__ __forceinline__ double cvt(R v) { return double(v); }
     template <class Real> static __device__ __forceinline__ Real to(double v, double) { return Real(v); }
     static __device__ __forceinline__ void add_shared(double *a, double v) { atomicAdd(a, v); }
-    static __device__ __forceinline__ void add_global(double *a, double v) { atomicAdd(a, v); }
+    static __device__ __forceinline__ void add_global(double *a, double v) { red_global_add(a, v); }
 };
 
 __device__ __forceinline__ void warp_flush_status(DevStatus *st, uint32_t err, uint32_t perr, int ndis)
@@ -569,12 +582,12 @@ __device__ __forceinline__ void patch_flush_rows(Patch<Real> &p, const Tile<Acc,
 // interleaved cell order) overlap in two node rows.  Each lane adds the
 // upper neighbour's lowest row and the lower neighbour's highest row into
 // its centre row with warp shuffles (a fixed order of float adds, so the
-// fixed-point sums stay deterministic), and only rows no neighbour took are
-// written out: in the usual case 9 of the 27 node-channel adds remain.
-// All 32 lanes of the warp must call it.
-template <class Real, class Acc, int CAP>
-__device__ __forceinline__ void patch_merge_flush(Patch<Real> &p, const Tile<Acc, CAP> &T, const AccGrid<Acc> &gacc, int gy,
-                                                  int lane)
+// fixed-point sums stay deterministic); `low` / `high` tell whether the
+// lane's own lowest / highest row is still its to write (no neighbour took
+// it).  In the usual case 9 of the 27 node-channel adds remain.  All 32
+// lanes of the warp must call it.
+template <class Real>
+__device__ __forceinline__ void patch_merge(Patch<Real> &p, int lane, bool &low, bool &high)
 {
     const unsigned FULL = 0xffffffffu;
     const bool mine = p.have && p.in_tile;
@@ -592,7 +605,42 @@ __device__ __forceinline__ void patch_merge_flush(Patch<Real> &p, const Tile<Acc
         if (above) { p.m[a][1] += um; p.px[a][1] += ux; p.py[a][1] += uy; }
         if (below) { p.m[a][1] += dm; p.px[a][1] += dx; p.py[a][1] += dy; }
     }
-    if (p.have) patch_flush_rows<Real, Acc, CAP>(p, T, gacc, gy, !below, !above);
+    low = !below;
+    high = !above;
+}
+
+// Adds a lane's end patch into the shared tile.  ATOMIC: shared atomics.
+// Otherwise plain read-add-write, which needs (a) no two lanes of the warp
+// on the same cell, so one (a, b) step of the warp touches distinct nodes,
+// (b) the steps separated by __syncwarp, since different lanes reach the
+// same node in different steps, and (c) no other warp writing the same nodes
+// meanwhile.  All 32 lanes of the warp must call the plain form.
+template <bool ATOMIC, class Real, class Acc, int CAP>
+__device__ __forceinline__ void patch_store(const Patch<Real> &p, const Tile<Acc, CAP> &T, bool on, bool low,
+                                            bool high)
+{
+    const int base = (p.cx - 1 - T.x0) * T.th + (p.cy - 1 - T.y0);
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int b = 0; b < 3; b++) {
+            if (on && (b != 0 || low) && (b != 2 || high)) {
+                const int li = base + a * T.th + b;
+                const Acc am = AccOps<Acc>::cvt(p.m[a][b]), ax = AccOps<Acc>::cvt(p.px[a][b]),
+                          ay = AccOps<Acc>::cvt(p.py[a][b]);
+                if (ATOMIC) {
+                    AccOps<Acc>::add_shared(&T.t[0][li], am);
+                    AccOps<Acc>::add_shared(&T.t[1][li], ax);
+                    AccOps<Acc>::add_shared(&T.t[2][li], ay);
+                } else {
+                    volatile Acc *t0 = &T.t[0][li], *t1 = &T.t[1][li], *t2 = &T.t[2][li];
+                    *t0 = *t0 + am;
+                    *t1 = *t1 + ax;
+                    *t2 = *t2 + ay;
+                }
+            }
+            if (!ATOMIC) __syncwarp();
+        }
 }
 
 // The node terms of src_terms, summed separably: with
@@ -667,6 +715,7 @@ template <class Real, class Acc, int BT, int PPT, int CAP, int STAGES> struct Ch
     Acc tile[3][CAP];
     unsigned long long mbar[2];
     int red[BT / 32][5];
+    int wbox[BT / 32][5];   // per warp: node box of its end patches {x0, x1, y0, y1}, duplicate cells
 };
 
 template <class Real, class Stage>
@@ -904,8 +953,57 @@ k_g2p_p2g(KParams<Real> kp, Pts<Real> P, Grid<Real, Acc> G, DevStatus *st, int n
                 }
             }
         }
-        patch_merge_flush<Real, Acc, CAP>(patch, T, G.acc, kp.gy, lane);
-        __syncthreads();
+        // end patches: merge neighbours, then write into the tile.  For int64
+        // accumulators (whose shared atomics are multi-instruction sequences)
+        // the writes go without atomics in two phases (even warps, odd warps)
+        // when warps of one phase touch disjoint nodes and no warp has two
+        // lanes on one cell; float accumulators keep the native atomics.
+        if (!AccOps<Acc>::fixed) {
+            bool low = true, high = true;
+            patch_merge(patch, lane, low, high);
+            if (patch.have) {
+                if (patch.in_tile) patch_store<true, Real, Acc, CAP>(patch, T, true, low, high);
+                else patch_flush<Real, Acc, CAP>(patch, T, G.acc, kp.gy);
+            }
+            __syncthreads();
+        } else {
+            const unsigned FULL = 0xffffffffu;
+            bool low = true, high = true;
+            patch_merge(patch, lane, low, high);
+            if (patch.have && !patch.in_tile) patch_flush<Real, Acc, CAP>(patch, T, G.acc, kp.gy);
+            const bool mine = patch.have;
+            const uint32_t key = mine ? (((uint32_t)patch.cx << 16) | (uint32_t)patch.cy) : (0xffffffe0u | (uint32_t)lane);
+            // every lane takes part in the match (a lane skipped here would stall the warp)
+            const unsigned same = __match_any_sync(FULL, key);
+            const bool dup = __any_sync(FULL, mine && __popc(same) > 1);
+            const int x0 = __reduce_min_sync(FULL, mine ? patch.cx - 1 : INT_MAX);
+            const int x1 = __reduce_max_sync(FULL, mine ? patch.cx + 1 : INT_MIN);
+            const int y0 = __reduce_min_sync(FULL, mine ? patch.cy - 1 : INT_MAX);
+            const int y1 = __reduce_max_sync(FULL, mine ? patch.cy + 1 : INT_MIN);
+            if (lane == 0) {
+                sm.wbox[wid][0] = x0; sm.wbox[wid][1] = x1; sm.wbox[wid][2] = y0; sm.wbox[wid][3] = y1;
+                sm.wbox[wid][4] = dup ? 1 : 0;
+            }
+            __syncthreads();
+            bool phased = true;
+#pragma unroll
+            for (int w = 0; w < NW; w++) {
+                if (sm.wbox[w][4]) phased = false;
+#pragma unroll
+                for (int v = w + 2; v < NW; v += 2)
+                    if (!(sm.wbox[w][1] < sm.wbox[v][0] || sm.wbox[v][1] < sm.wbox[w][0] ||
+                          sm.wbox[w][3] < sm.wbox[v][2] || sm.wbox[v][3] < sm.wbox[w][2]))
+                        phased = false;
+            }
+            if (phased) {
+                if ((wid & 1) == 0) patch_store<false, Real, Acc, CAP>(patch, T, mine, low, high);
+                __syncthreads();
+                if ((wid & 1) == 1) patch_store<false, Real, Acc, CAP>(patch, T, mine, low, high);
+            } else if (mine) {
+                patch_store<true, Real, Acc, CAP>(patch, T, true, low, high);
+            }
+            __syncthreads();
+        }
         // one stage: its points are all read now, fetch the next chunk into it
         if (STAGES == 1 && tid == 0 && c + (int)gridDim.x < nchunks)
             fetch_chunk(sm.stage[0], P, (uint32_t)(c + (int)gridDim.x) * CH, CH, &sm.mbar[0]);

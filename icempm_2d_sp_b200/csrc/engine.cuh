@@ -38,6 +38,7 @@
 #include <type_traits>
 #include <cuda_runtime.h>
 #include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
 
 #include "device_math.cuh"
 #include "icempm.h"

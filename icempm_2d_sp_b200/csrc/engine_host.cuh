@@ -57,7 +57,10 @@ public:
         ICEMPM_CUDA(cudaEventCreate(&evs_[1]));
         ICEMPM_CUDA(cudaEventCreate(&evs_[2]));
         // points, two parities for the sort gather
-        const size_t nc = ((size_t)cap_ + PAD - 1) / PAD * PAD;   // the bulk copies read whole chunks
+        // room for the cell padding of the locality order (a quarter more), in
+        // whole chunks (the bulk copies read whole chunks)
+        const size_t nc = ((size_t)cap_ + cap_ / 4 + 4 * PAD + PAD - 1) / PAD * PAD;
+        nc_ = nc;
         const size_t per = nc * (3 * sizeof(V4<Real>) + 2 * sizeof(V2<Real>) + sizeof(uint2) + 2 * sizeof(uint32_t) + sizeof(double));
         ICEMPM_CUDA(cudaMalloc(&pts_mem_, 2 * per));
         for (int par = 0; par < 2; par++) {
@@ -95,12 +98,17 @@ public:
         ICEMPM_CUDA(cudaMalloc(&keys_[1], nc * sizeof(uint64_t)));
         ICEMPM_CUDA(cudaMalloc(&vals_[0], nc * sizeof(uint32_t)));
         ICEMPM_CUDA(cudaMalloc(&vals_[1], nc * sizeof(uint32_t)));
+        ICEMPM_CUDA(cudaMalloc(&runs_, nc * sizeof(uint32_t)));
+        ICEMPM_CUDA(cudaMalloc(&aux_, 8 * sizeof(int)));
         size_t t32 = 0, t64 = 0;
         ICEMPM_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, t32, (uint32_t *)nullptr, (uint32_t *)nullptr,
                                                     (uint32_t *)nullptr, (uint32_t *)nullptr, (int)nc, 0, 32, stream_));
         ICEMPM_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, t64, (uint64_t *)nullptr, (uint64_t *)nullptr,
                                                     (uint32_t *)nullptr, (uint32_t *)nullptr, (int)nc, 0, 64, stream_));
-        sort_tmp_bytes_ = std::max(t32, t64);
+        size_t ts1 = 0, ts2 = 0;
+        ICEMPM_CUDA(cub::DeviceScan::InclusiveSum(nullptr, ts1, (uint32_t *)nullptr, (uint32_t *)nullptr, (int)nc, stream_));
+        ICEMPM_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, ts2, (uint32_t *)nullptr, (uint32_t *)nullptr, (int)nc, stream_));
+        sort_tmp_bytes_ = std::max(std::max(t32, t64), std::max(ts1, ts2));
         ICEMPM_CUDA(cudaMalloc(&sort_tmp_, sort_tmp_bytes_));
         // a CTA of the fused kernel handles BT*PPT points, ~BT*PPT/4 cells at
         // 4 points per cell: 8 columns of BT*PPT/32 cells
@@ -218,6 +226,7 @@ public:
             launches_++;
         }
         n_ = n;
+        n_real_ = n;
         double mt = 0;
         for (uint32_t i = 0; i < n; i++) mt = std::max(mt, std::fabs(hssoa[(size_t)18 * host_cap + i]));
         set_params(prms_, mt > 0 ? mt : 1.0);
@@ -235,18 +244,18 @@ public:
 
     int download(double *hssoa, uint32_t host_cap, uint32_t *size) override
     {
-        if (n_ > host_cap) return fail(ICEMPM_E_CAPACITY, "host buffer capacity is smaller than the point count");
+        if (n_real_ > host_cap) return fail(ICEMPM_E_CAPACITY, "host buffer capacity is smaller than the point count");
         int rc = ensure_stage();
         if (rc) return rc;
         if (n_ > 0) {
-            k_download<Real><<<(n_ + 255) / 256, 256, 0, stream_>>>(pts_[par_], (int)n_, stage_, n_);
+            k_download<Real><<<(n_ + 255) / 256, 256, 0, stream_>>>(pts_[par_], (int)n_, stage_, n_real_);
             ICEMPM_CUDA(cudaGetLastError());
             launches_++;
-            ICEMPM_CUDA(cudaMemcpy2DAsync(hssoa, (size_t)host_cap * sizeof(double), stage_, (size_t)n_ * sizeof(double),
-                                          (size_t)n_ * sizeof(double), ICEMPM_N_PTS_ARRAYS, cudaMemcpyDeviceToHost, stream_));
+            ICEMPM_CUDA(cudaMemcpy2DAsync(hssoa, (size_t)host_cap * sizeof(double), stage_, (size_t)n_real_ * sizeof(double),
+                                          (size_t)n_real_ * sizeof(double), ICEMPM_N_PTS_ARRAYS, cudaMemcpyDeviceToHost, stream_));
         }
         ICEMPM_CUDA(cudaStreamSynchronize(stream_));
-        if (size) *size = n_;
+        if (size) *size = n_real_;
         return 0;
     }
 
@@ -442,21 +451,70 @@ public:
     }
 
     // Sort by the tiled locality key into the other parity, in the fused
-    // kernel's interleaved order (host slots unchanged).
+    // kernel's interleaved order (host slots unchanged).  Each cell's run of
+    // enabled points is padded to a multiple of four with placeholders when
+    // the padded order fits the arrays; the placeholders of an earlier padding
+    // are dropped first (they sort last).
     int locality_sort()
     {
         if (n_ == 0) return 0;
         const unsigned nb = (n_ + 255) / 256;
         uint32_t *k32in = (uint32_t *)keys_[0], *k32out = (uint32_t *)keys_[1];
-        k_keys_tiled<<<nb, 256, 0, stream_>>>(pts_[par_].K, (int)n_, tile_, k32in, vals_[0]);
+        k_keys_tiled<<<nb, 256, 0, stream_>>>(pts_[par_].K, pts_[par_].slot, (int)n_, tile_, k32in, vals_[0]);
         launches_++;
         size_t tb = sort_tmp_bytes_;
         ICEMPM_CUDA(cub::DeviceRadixSort::SortPairs(sort_tmp_, tb, k32in, k32out, vals_[0], vals_[1], (int)n_, 0, 32, stream_));
         launches_ += 4;
-        k_gather<Real><<<nb, 256, 0, stream_>>>(pts_[par_], pts_[1 - par_], vals_[1], (int)n_, 0, PPT);
+        k_key_bounds<<<(n_ + 256) / 256, 256, 0, stream_>>>(k32out, (int)n_, aux_);
         launches_++;
+        int bounds[2] = {0, 0};
+        ICEMPM_CUDA(cudaMemcpyAsync(bounds, aux_, sizeof(bounds), cudaMemcpyDeviceToHost, stream_));
+        ICEMPM_CUDA(cudaStreamSynchronize(stream_));
+        const uint32_t n_en = (uint32_t)bounds[0], n_real = (uint32_t)bounds[1];
+        // run bookkeeping in the free halves of the key buffers and vals_[0]
+        uint32_t *flags = k32in, *run_id = k32in + nc_, *begin = k32out + nc_, *padded = vals_[0], *pstart = runs_;
+        uint32_t n_pad = n_real, n_pad_en = n_en;
+        int runs = 0;
+        if (n_en > 0) {
+            const unsigned nbe = (n_en + 255) / 256;
+            k_run_flags<<<nbe, 256, 0, stream_>>>(k32out, (int)n_en, flags);
+            tb = sort_tmp_bytes_;
+            ICEMPM_CUDA(cub::DeviceScan::InclusiveSum(sort_tmp_, tb, flags, run_id, (int)n_en, stream_));
+            k_run_begin<<<nbe, 256, 0, stream_>>>(run_id, (int)n_en, begin);
+            launches_ += 3;
+            uint32_t r = 0;
+            ICEMPM_CUDA(cudaMemcpyAsync(&r, run_id + n_en - 1, sizeof(r), cudaMemcpyDeviceToHost, stream_));
+            ICEMPM_CUDA(cudaStreamSynchronize(stream_));
+            runs = (int)r;
+            k_run_padded<<<(runs + 255) / 256, 256, 0, stream_>>>(begin, runs, (int)n_en, padded);
+            tb = sort_tmp_bytes_;
+            ICEMPM_CUDA(cub::DeviceScan::ExclusiveSum(sort_tmp_, tb, padded, pstart, runs, stream_));
+            launches_ += 2;
+            uint32_t last[2] = {0, 0};
+            ICEMPM_CUDA(cudaMemcpyAsync(&last[0], pstart + runs - 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream_));
+            ICEMPM_CUDA(cudaMemcpyAsync(&last[1], padded + runs - 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream_));
+            ICEMPM_CUDA(cudaStreamSynchronize(stream_));
+            n_pad_en = last[0] + last[1];
+            n_pad = n_pad_en + (n_real - n_en);
+            if ((size_t)n_pad > nc_) {   // does not fit: unpadded order
+                n_pad = n_real; n_pad_en = n_en; runs = 0;
+            }
+        }
+        if (runs > 0) {
+            k_gather_padded<Real><<<(n_real + 255) / 256, 256, 0, stream_>>>(
+                pts_[par_], pts_[1 - par_], vals_[1], (int)n_real, n_en, n_pad_en, n_pad, run_id, begin, pstart, PPT);
+            k_fill_placeholders<Real><<<(runs + 255) / 256, 256, 0, stream_>>>(pts_[1 - par_], runs, n_en, n_pad, begin,
+                                                                              pstart, padded, PPT);
+            launches_ += 2;
+        } else if (n_real > 0) {
+            k_gather<Real><<<(n_real + 255) / 256, 256, 0, stream_>>>(pts_[par_], pts_[1 - par_], vals_[1],
+                                                                     (int)n_real, 0, PPT);
+            launches_++;
+        }
         ICEMPM_CUDA(cudaGetLastError());
         par_ = 1 - par_;
+        n_ = n_pad;
+        n_real_ = n_real;
         steps_since_sort_ = 0;
         invalidate_graphs();
         return 0;
@@ -481,6 +539,7 @@ public:
             ICEMPM_CUDA(cudaMemcpyAsync(&s, st_, sizeof(s), cudaMemcpyDeviceToHost, stream_));
             ICEMPM_CUDA(cudaStreamSynchronize(stream_));
             n_ = (uint32_t)s.n_active;
+            n_real_ = n_;
         }
         const int32_t zero = 0;
         ICEMPM_CUDA(cudaMemcpyAsync(&st_->disabled, &zero, sizeof(zero), cudaMemcpyHostToDevice, stream_));
@@ -490,7 +549,7 @@ public:
         return locality_sort();
     }
 
-    uint32_t count() const override { return n_; }
+    uint32_t count() const override { return n_real_; }
     cudaStream_t stream() const override { return stream_; }
     uint64_t launches() const override { return launches_; }
     double fixed_scale_m() const override { return kp_.scale_m; }
@@ -513,7 +572,7 @@ private:
         invalidate_graphs();
         cudaFree(pts_mem_); cudaFree(acc_); cudaFree(vel_); cudaFree(cur_); cudaFree(frc_); cudaFree(status_);
         cudaFree(force_); cudaFree(st_); cudaFree(stage_); cudaFree(keys_[0]); cudaFree(keys_[1]);
-        cudaFree(vals_[0]); cudaFree(vals_[1]); cudaFree(sort_tmp_);
+        cudaFree(vals_[0]); cudaFree(vals_[1]); cudaFree(sort_tmp_); cudaFree(runs_); cudaFree(aux_);
         if (ev0_) cudaEventDestroy(ev0_);
         if (ev1_) cudaEventDestroy(ev1_);
         for (auto &e : evs_) if (e) cudaEventDestroy(e);
@@ -525,7 +584,10 @@ private:
     icempm_options_t opts_{};
     int gx_ = 0, gy_ = 0;
     size_t G_ = 0;
-    uint32_t cap_ = 0, n_ = 0;
+    uint32_t cap_ = 0;
+    uint32_t n_ = 0;        // entries of the point arrays the kernels walk (points + placeholders)
+    uint32_t n_real_ = 0;   // points (host slots)
+    size_t nc_ = 0;         // allocated entries per point array
     double max_thick_ = 1.0;
     cudaStream_t stream_ = nullptr;
     cudaEvent_t ev0_ = nullptr, ev1_ = nullptr, evs_[3] = {nullptr, nullptr, nullptr};
@@ -541,6 +603,8 @@ private:
     double *stage_ = nullptr;
     uint64_t *keys_[2] = {nullptr, nullptr};
     uint32_t *vals_[2] = {nullptr, nullptr};
+    uint32_t *runs_ = nullptr;   // padded run starts of the locality order
+    int *aux_ = nullptr;         // small device results read back by the host
     void *sort_tmp_ = nullptr;
     size_t sort_tmp_bytes_ = 0;
     TileKey tile_{8, 8, 1};

@@ -29,12 +29,18 @@ __global__ void k_upload(const double *__restrict__ stage, size_t pitch, int n, 
     P.thick64[i] = r[18 * pitch];
 }
 
+// Slot of a placeholder point (cell padding of the locality order): it
+// belongs to no host slot and is never written back.
+constexpr uint32_t kSlotNone = 0xffffffffu;
+
 template <class Real>
 __global__ void k_download(Pts<Real> P, int n, double *__restrict__ stage, size_t pitch)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const size_t s = P.slot[i];
+    const uint32_t s32 = P.slot[i];
+    if (s32 == kSlotNone) return;
+    const size_t s = s32;
     double *r = stage + s;
     const V4<Real> A = P.A[i], H = P.H[i], C = P.C[i];
     const V2<Real> V = P.V[i], PQ = P.PQ[i];
@@ -51,15 +57,18 @@ __global__ void k_download(Pts<Real> P, int n, double *__restrict__ stage, size_
 
 // ---- sorting ---------------------------------------------------------------
 // Locality key: cells grouped in TX x TY tiles, tiles in column order, cells
-// column-major inside a tile; disabled points sort last.
+// column-major inside a tile; disabled points sort after the enabled ones and
+// placeholders last.
 struct TileKey { int tx, ty, ntiles_y; };
-static __global__ void k_keys_tiled(const uint2 *__restrict__ K, int n, TileKey t, uint32_t *keys, uint32_t *vals)
+constexpr uint32_t kKeyDisabled = 0xfffffffeu, kKeyPlaceholder = 0xffffffffu;
+static __global__ void k_keys_tiled(const uint2 *__restrict__ K, const uint32_t *__restrict__ slot, int n, TileKey t,
+                                    uint32_t *keys, uint32_t *vals)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const uint2 k = K[i];
-    uint32_t key = 0xffffffffu;
-    if (!(k.y & kDisabled)) {
+    uint32_t key = slot[i] == kSlotNone ? kKeyPlaceholder : kKeyDisabled;
+    if (key == kKeyDisabled && !(k.y & kDisabled)) {
         const uint32_t cx = k.x & 0xffffu, cy = k.x >> 16;
         const uint32_t tile = (cx / t.tx) * (uint32_t)t.ntiles_y + cy / t.ty;
         key = tile * (uint32_t)(t.tx * t.ty) + (cx % t.tx) * t.ty + cy % t.ty;
@@ -113,6 +122,101 @@ __global__ void k_gather(Pts<Real> src, Pts<Real> dst, const uint32_t *__restric
     dst.slot[i] = reslot ? (uint32_t)r : src.slot[j];
     dst.pid[i] = src.pid[j];
     dst.thick64[i] = src.thick64[j];
+}
+
+// ---- cell-aligned padding of the locality order ------------------------------
+// The fused kernel gives each thread PPT consecutive points.  With four points
+// per cell, padding every cell's run of points to a multiple of four with
+// disabled placeholders puts each thread's points in one cell, which is what
+// lets neighbouring threads merge their scatter patches and write them
+// without shared atomics.  Runs are found on the sorted keys: start flags,
+// an inclusive scan numbers the runs, each run's padded length is scanned to
+// its padded start.
+
+// first index whose key reaches each bound: bounds[0] = enabled count,
+// bounds[1] = enabled + disabled count (keys sorted ascending)
+static __global__ void k_key_bounds(const uint32_t *__restrict__ keys, int n, int *bounds)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i > n) return;
+    const uint32_t prev = i == 0 ? 0u : keys[i - 1];
+    const uint32_t cur = i == n ? kKeyPlaceholder : keys[i];
+    const bool prev_en = i > 0 && prev < kKeyDisabled, cur_en = i < n && cur < kKeyDisabled;
+    const bool prev_real = i > 0 && prev != kKeyPlaceholder, cur_real = i < n && cur != kKeyPlaceholder;
+    if ((i == 0 || prev_en) && !cur_en) bounds[0] = i;
+    if ((i == 0 || prev_real) && !cur_real) bounds[1] = i;
+}
+
+static __global__ void k_run_flags(const uint32_t *__restrict__ keys, int n, uint32_t *flags)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    flags[i] = (i == 0 || keys[i] != keys[i - 1]) ? 1u : 0u;
+}
+
+// run_id: inclusive scan of the flags (1-based run number of each entry)
+static __global__ void k_run_begin(const uint32_t *__restrict__ run_id, int n, uint32_t *begin)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (i == 0 || run_id[i] != run_id[i - 1]) begin[run_id[i] - 1] = (uint32_t)i;
+}
+
+static __global__ void k_run_padded(const uint32_t *__restrict__ begin, int runs, int n, uint32_t *padded)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= runs) return;
+    const uint32_t end = s + 1 < runs ? begin[s + 1] : (uint32_t)n;
+    padded[s] = (end - begin[s] + 3u) & ~3u;
+}
+
+// Padded rank of sorted rank r: enabled points at their run's padded start
+// plus their offset in the run, disabled points after all padded runs.
+__device__ __forceinline__ size_t padded_rank(uint32_t r, uint32_t n_en, uint32_t n_pad_en,
+                                              const uint32_t *__restrict__ run_id, const uint32_t *__restrict__ begin,
+                                              const uint32_t *__restrict__ pstart)
+{
+    if (r >= n_en) return (size_t)n_pad_en + (r - n_en);
+    const uint32_t s = run_id[r] - 1;
+    return (size_t)pstart[s] + (r - begin[s]);
+}
+
+// dst[interleaved(padded_rank(r))] = src[perm[r]] for the n_real real points
+template <class Real>
+__global__ void k_gather_padded(Pts<Real> src, Pts<Real> dst, const uint32_t *__restrict__ perm, int n_real,
+                                uint32_t n_en, uint32_t n_pad_en, uint32_t n_pad, const uint32_t *__restrict__ run_id,
+                                const uint32_t *__restrict__ begin, const uint32_t *__restrict__ pstart, int ppt)
+{
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n_real) return;
+    const uint32_t j = perm[r];
+    const size_t i = interleaved_position(padded_rank((uint32_t)r, n_en, n_pad_en, run_id, begin, pstart), n_pad, ppt);
+    dst.A[i] = src.A[j]; dst.H[i] = src.H[j]; dst.C[i] = src.C[j];
+    dst.V[i] = src.V[j]; dst.PQ[i] = src.PQ[j]; dst.K[i] = src.K[j];
+    dst.slot[i] = src.slot[j];
+    dst.pid[i] = src.pid[j];
+    dst.thick64[i] = src.thick64[j];
+}
+
+// placeholders in the padding of each run (at most three per run)
+template <class Real>
+__global__ void k_fill_placeholders(Pts<Real> dst, int runs, uint32_t n_en, uint32_t n_pad, const uint32_t *__restrict__ begin,
+                                    const uint32_t *__restrict__ pstart, const uint32_t *__restrict__ padded, int ppt)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= runs) return;
+    const uint32_t end = s + 1 < runs ? begin[s + 1] : n_en;
+    const uint32_t cnt = end - begin[s];
+    for (uint32_t k = cnt; k < padded[s]; k++) {
+        const size_t i = interleaved_position((size_t)pstart[s] + k, n_pad, ppt);
+        V4<Real> z; z.x = z.y = z.z = z.w = Real(0);
+        V2<Real> z2; z2.x = z2.y = Real(0);
+        dst.A[i] = z; dst.H[i] = z; dst.C[i] = z; dst.V[i] = z2; dst.PQ[i] = z2;
+        dst.K[i] = make_uint2(0u, kDisabled);
+        dst.slot[i] = kSlotNone;
+        dst.pid[i] = 0u;
+        dst.thick64[i] = 0.0;
+    }
 }
 
 // number of leading keys that are not ~0 (keys sorted ascending)

@@ -51,6 +51,9 @@ B_POINT, B_NODE = 124, 49
 # split of the node bytes: the fused G2P+P2G kernel reads 8 B of velocity and
 # flushes 12 B of accumulators per node; the grid update moves the other 29 B
 B_NODE_FUSED = 20
+# measured DRAM traffic of the fused kernel per point, grid share included
+# (489.08 MB for 5,884,928 points and 2,097,152 nodes in one launch)
+TRAFFIC_B_PER_POINT = 83.11
 
 
 def parse():
@@ -300,12 +303,10 @@ def main():
     fused_bytes = B_POINT * n + B_NODE_FUSED * G
     fused_launch_s = fused * 1e-3 / args.steps
     achieved = fused_bytes / fused_launch_s / 1e9
-    traffic = None
-    tp = os.path.join(ROOT, "profiles", "fused_kernel_traffic.json")
-    if os.path.exists(tp):
-        with open(tp) as f:
-            td = json.load(f)
-        traffic = td["bytes_per_point"] * n + td["bytes_per_node"] * G
+    # DRAM bytes of one fused launch from an ncu capture (dram__bytes_read.sum +
+    # dram__bytes_write.sum of profiles/k_g2p_p2g_config1_2048x1024.md), per
+    # point, scaled to this scene's point count (same node/point ratio)
+    traffic = TRAFFIC_B_PER_POINT * n
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": traffic, "peak_source": peak_src,
                 "kernel": "k_g2p_p2g (fused G2P + P2G)", "algorithmic_bytes_per_launch": fused_bytes,

@@ -224,19 +224,43 @@ def cpu_baseline(args, sc):
             "sample": f"the full benchmark scene (N={sc.n}) for {k} sub-steps with the FP64 OpenMP oracle"}
 
 
+def init_ranks(world, local):
+    """One process per GPU under torchrun: NCCL where CUDA is present, gloo on
+    CPU-only hosts (the host-side reference arm and the tests).  Returns the
+    torch.distributed module, or None for a single process."""
+    if world <= 1:
+        return None
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    if torch.cuda.is_available():
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+    else:
+        dist.init_process_group("gloo", timeout=timedelta(seconds=600))
+    return dist
+
+
+def combine_ranks(dist, t_ms, n):
+    """Whole-job figures from per-rank ones: the slowest rank's time and the
+    points of all ranks (each rank advances its own scene: weak scaling)."""
+    if dist is None:
+        return t_ms, n
+    import torch
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(t_ms)], device=dev, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    c = torch.tensor([float(n)], device=dev, dtype=torch.float64)
+    dist.all_reduce(c, op=dist.ReduceOp.SUM)
+    return float(t.item()), int(c.item())
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    dist = None
-    if world > 1:
-        import torch
-        import torch.distributed as dist
-        from datetime import timedelta
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=timedelta(seconds=600),
-                                device_id=torch.device("cuda", local))
+    dist = init_ranks(world, local)
     if args.impl == "reference":
         run_reference(args, rank)
         if dist:
@@ -282,15 +306,7 @@ def main():
         return total, upd, fused, launches, sampler.summary(t0, t1), err
 
     total, upd, fused, launches, clocks, err = timed(VARIANT_FIXED)
-    t_ms = total
-    n_tot = n
-    if dist:
-        t = torch.tensor([t_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_ms = float(t.item())
-        c = torch.tensor([float(n)], device="cuda", dtype=torch.float64)
-        dist.all_reduce(c, op=dist.ReduceOp.SUM)
-        n_tot = int(c.item())
+    t_ms, n_tot = combine_ranks(dist, total, n)
     value = n_tot * args.steps / (t_ms * 1e-3)
 
     plain = None

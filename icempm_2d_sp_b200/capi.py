@@ -20,7 +20,19 @@ EXPORTS = [
     "icempm_sort_compact", "icempm_timings", "icempm_phase_times", "icempm_fixed_point_scales",
     "icempm_host_register", "icempm_host_unregister", "icempm_device_count", "icempm_point_count",
     "icempm_get_stream", "icempm_launch_count", "icempm_last_error", "icempm_cell_order_noalloc",
+    "icempm_batch_create", "icempm_batch_destroy", "icempm_batch_step", "icempm_batch_autotune",
+    "icempm_batch_set_tuning", "icempm_batch_get_tuning", "icempm_batch_timings", "icempm_batch_launch_count",
 ]
+
+
+class BatchTuning(C.Structure):
+    """icempm_batch_tuning_t"""
+    _fields_ = [("tile_nodes", C.c_int32), ("stages", C.c_int32), ("sort_every", C.c_int32),
+                ("graph_steps", C.c_int32), ("ms_per_step", C.c_float), ("reserved", C.c_int32 * 3)]
+
+    def as_dict(self):
+        return {"tile_nodes": self.tile_nodes, "stages": self.stages, "sort_every": self.sort_every,
+                "graph_steps": self.graph_steps, "ms_per_step": self.ms_per_step}
 
 
 class IcempmError(RuntimeError):
@@ -68,6 +80,14 @@ def load(path: str = LIB_PATH):
         "icempm_last_error": (C.c_char_p, []),
         "icempm_cell_order_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_int32,
                                                 C.c_void_p, C.c_void_p, C.c_void_p]),
+        "icempm_batch_create": (C.c_int, [C.POINTER(h), C.c_int32, C.POINTER(h)]),
+        "icempm_batch_destroy": (C.c_int, [h]),
+        "icempm_batch_step": (C.c_int, [h, C.c_int32, C.c_int32]),
+        "icempm_batch_autotune": (C.c_int, [h, C.c_int32, C.c_int32, C.POINTER(BatchTuning)]),
+        "icempm_batch_set_tuning": (C.c_int, [h, C.POINTER(BatchTuning)]),
+        "icempm_batch_get_tuning": (C.c_int, [h, C.POINTER(BatchTuning)]),
+        "icempm_batch_timings": (C.c_int, [h, C.POINTER(C.c_float)]),
+        "icempm_batch_launch_count": (C.c_int, [h, C.POINTER(C.c_uint64)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -208,3 +228,61 @@ class Context:
         c = C.c_uint64(0)
         check(self._L.icempm_launch_count(self.h, C.byref(c)))
         return c.value
+
+
+class Batch:
+    """Ensemble of contexts (same variant, same device) advanced together:
+    one launch of each kernel per sub-step for all scenes.  The contexts must
+    outlive the batch."""
+
+    def __init__(self, contexts):
+        L = load()
+        self._L = L
+        self.contexts = list(contexts)
+        arr = (C.c_void_p * max(1, len(self.contexts)))(*[c.h.value for c in self.contexts])
+        h = C.c_void_p()
+        check(L.icempm_batch_create(C.cast(arr, C.POINTER(C.c_void_p)), len(self.contexts), C.byref(h)))
+        self.h = h
+
+    def step(self, nsteps, first_step=0):
+        check(self._L.icempm_batch_step(self.h, int(nsteps), int(first_step)))
+
+    def autotune(self, trial_steps=100, first_step=0):
+        t = BatchTuning()
+        check(self._L.icempm_batch_autotune(self.h, int(trial_steps), int(first_step), C.byref(t)))
+        return t
+
+    def set_tuning(self, tuning):
+        check(self._L.icempm_batch_set_tuning(self.h, C.byref(tuning)))
+
+    def tuning(self):
+        t = BatchTuning()
+        check(self._L.icempm_batch_get_tuning(self.h, C.byref(t)))
+        return t
+
+    def timings(self):
+        ms = (C.c_float * 4)()
+        check(self._L.icempm_batch_timings(self.h, ms))
+        return list(ms)
+
+    def launch_count(self):
+        v = C.c_uint64()
+        check(self._L.icempm_batch_launch_count(self.h, C.byref(v)))
+        return v.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            self._L.icempm_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

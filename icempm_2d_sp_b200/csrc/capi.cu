@@ -5,6 +5,7 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <vector>
 
 #include "engine_iface.h"
 
@@ -24,6 +25,13 @@ struct icempm_context {
     icempm_simparams_t prms{};
     icempm_options_t opts{};
 };
+
+struct icempm_batch {
+    icempm::Batch *b = nullptr;
+};
+
+#define ICEMPM_GUARD_BATCH(bt) \
+    if (!(bt) || !(bt)->b) return fail(ICEMPM_E_ARG, "null batch")
 
 #define ICEMPM_GUARD_CTX(ctx) \
     if (!(ctx) || !(ctx)->eng) return fail(ICEMPM_E_ARG, "null context")
@@ -231,6 +239,86 @@ int icempm_device_count(int *count)
     if (!count) return fail(ICEMPM_E_ARG, "count is null");
     cudaError_t e = cudaGetDeviceCount(count);
     if (e != cudaSuccess) { *count = 0; return fail(ICEMPM_E_CUDA, cudaGetErrorString(e)); }
+    return ICEMPM_OK;
+}
+
+int icempm_batch_create(icempm_t *const *contexts, int32_t count, icempm_batch_t **out)
+{
+    if (!out) return fail(ICEMPM_E_ARG, "out is null");
+    *out = nullptr;
+    if (!contexts || count < 1) return fail(ICEMPM_E_ARG, "at least one context is required");
+    std::vector<icempm::Engine *> eng((size_t)count);
+    for (int i = 0; i < count; i++) {
+        if (!contexts[i] || !contexts[i]->eng) return fail(ICEMPM_E_ARG, "null context in the batch");
+        if (contexts[i]->opts.variant != contexts[0]->opts.variant)
+            return fail(ICEMPM_E_ARG, "all contexts of a batch must use the same variant");
+        eng[i] = contexts[i]->eng;
+    }
+    icempm::Batch *b = nullptr;
+    try {
+        switch (contexts[0]->opts.variant) {
+        case ICEMPM_VARIANT_FIXED: b = icempm::make_batch_fixed(eng.data(), count); break;
+        case ICEMPM_VARIANT_FP32: b = icempm::make_batch_fp32(eng.data(), count); break;
+        case ICEMPM_VARIANT_FP64: b = icempm::make_batch_fp64(eng.data(), count); break;
+        default: return fail(ICEMPM_E_ARG, "unknown variant");
+        }
+    } catch (const std::bad_alloc &) {
+        return fail(ICEMPM_E_NOMEM, "host allocation failed");
+    }
+    if (!b) return ICEMPM_E_STATE;
+    icempm_batch *bt = new (std::nothrow) icempm_batch;
+    if (!bt) { delete b; return fail(ICEMPM_E_NOMEM, "batch allocation failed"); }
+    bt->b = b;
+    *out = bt;
+    return ICEMPM_OK;
+}
+
+int icempm_batch_destroy(icempm_batch_t *batch)
+{
+    if (!batch) return ICEMPM_OK;
+    delete batch->b;
+    delete batch;
+    return ICEMPM_OK;
+}
+
+int icempm_batch_step(icempm_batch_t *batch, int32_t nsteps, int32_t first_step)
+{
+    ICEMPM_GUARD_BATCH(batch);
+    ICEMPM_TRY(batch->b->step(nsteps, first_step));
+}
+
+int icempm_batch_autotune(icempm_batch_t *batch, int32_t trial_steps, int32_t first_step, icempm_batch_tuning_t *out)
+{
+    ICEMPM_GUARD_BATCH(batch);
+    ICEMPM_TRY(batch->b->autotune(trial_steps, first_step, out));
+}
+
+int icempm_batch_set_tuning(icempm_batch_t *batch, const icempm_batch_tuning_t *tuning)
+{
+    ICEMPM_GUARD_BATCH(batch);
+    if (!tuning) return fail(ICEMPM_E_ARG, "tuning is null");
+    ICEMPM_TRY(batch->b->set_tuning(tuning));
+}
+
+int icempm_batch_get_tuning(icempm_batch_t *batch, icempm_batch_tuning_t *tuning)
+{
+    ICEMPM_GUARD_BATCH(batch);
+    if (!tuning) return fail(ICEMPM_E_ARG, "tuning is null");
+    ICEMPM_TRY(batch->b->get_tuning(tuning));
+}
+
+int icempm_batch_timings(icempm_batch_t *batch, float ms[4])
+{
+    ICEMPM_GUARD_BATCH(batch);
+    if (!ms) return fail(ICEMPM_E_ARG, "ms is null");
+    ICEMPM_TRY(batch->b->timings(ms));
+}
+
+int icempm_batch_launch_count(icempm_batch_t *batch, uint64_t *count)
+{
+    ICEMPM_GUARD_BATCH(batch);
+    if (!count) return fail(ICEMPM_E_ARG, "count is null");
+    *count = batch->b->launches();
     return ICEMPM_OK;
 }
 

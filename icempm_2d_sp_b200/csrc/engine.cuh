@@ -434,16 +434,11 @@ __global__ void __launch_bounds__(BT) k_p2g(KParams<Real> kp, Pts<Real> P, Grid<
 // ---- grid update (partition_kernel_update_nodes, kernels.cuh:109-177) ----
 // Compat forcing follows the reference; the extended forcing's stresses are
 // point impulses (make_src), so its node update is v = p/m with walls and clamp.
+// One node of the update; `step` is the sub-step index (the compat current ramp).
 template <class Real, class Acc, bool EXT>
-__global__ void __launch_bounds__(256) k_grid_update(KParams<Real> kp, Grid<Real, Acc> G, DevStatus *st,
-                                                     long long nnodes)
+__device__ __forceinline__ void grid_update_node(const KParams<Real> &kp, const Grid<Real, Acc> &G, DevStatus *st,
+                                                 long long idx, int step)
 {
-    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx == 0) {   // this step's scatter errors become visible now, as in the reference
-        const uint32_t pe = st->err_pending;
-        if (pe) { atomicOr(&st->err, pe); st->err_pending = 0; }
-    }
-    if (idx >= nnodes) return;
     struct { Acc m, px, py; } r = {G.acc.m[idx], G.acc.px[idx], G.acc.py[idx]};
     V2<Real> out;
     out.x = Real(0); out.y = Real(0);
@@ -465,7 +460,7 @@ __global__ void __launch_bounds__(256) k_grid_update(KParams<Real> kp, Grid<Real
             G.force[idx] = f;
         } else if (!EXT) {
             const V2<Real> c = G.cur[idx];
-            const double t = (double)(float)(kp.dt_d * (double)st->step);
+            const double t = (double)(float)(kp.dt_d * (double)step);
             const double ramp = (t < 300000) ? 1 + fmin(t / (3600 * 2), 2.) : 3 + fmin((t - 300000) / (3600 * 10), 2.);
             const Real wx = c.x * Real(ramp), wy = c.y * Real(ramp);
             const Real ux = wx - vx, uy = wy - vy;
@@ -480,6 +475,23 @@ __global__ void __launch_bounds__(256) k_grid_update(KParams<Real> kp, Grid<Real
     }
     G.vel[idx] = out;
     if (err) atomicOr(&st->err, err);
+}
+
+// this step's scatter errors become visible now, as in the reference
+__device__ __forceinline__ void fold_pending(DevStatus *st)
+{
+    const uint32_t pe = st->err_pending;
+    if (pe) { atomicOr(&st->err, pe); st->err_pending = 0; }
+}
+
+template <class Real, class Acc, bool EXT>
+__global__ void __launch_bounds__(256) k_grid_update(KParams<Real> kp, Grid<Real, Acc> G, DevStatus *st,
+                                                     long long nnodes)
+{
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx == 0) fold_pending(st);
+    if (idx >= nnodes) return;
+    grid_update_node<Real, Acc, EXT>(kp, G, st, idx, st->step);
 }
 
 // ---- fused G2P (step k) + P2G (step k+1) -----------------------------------
@@ -749,6 +761,248 @@ __device__ __forceinline__ void fetch_chunk(Stage &sg, const Pts<Real> &P, uint3
 // accumulators.  Every point of a chunk is read and written by the same
 // thread, so a stage can be refilled as soon as the CTA has passed the
 // barrier after its points.
+// One chunk of the fused kernel: CH = BT*PPT entries starting at `base` of a
+// scene's arrays, whose A, H, K are in stage `s`.  With one stage, the next
+// chunk (`next`, arrays Pn from base_n) is fetched into it once its points
+// are read.  Error bits and the count of newly disabled points accumulate
+// into err, perr, ndis.
+template <class Real, class Acc, int BT, int PPT, int CAP, int STAGES>
+__device__ __forceinline__ void fused_chunk(ChunkSmem<Real, Acc, BT, PPT, CAP, STAGES> &sm, int s,
+                                            const KParams<Real> &kp, const Pts<Real> &P, const Grid<Real, Acc> &G,
+                                            uint32_t base, int n, bool recordPQ, bool store_vc, bool next,
+                                            const Pts<Real> &Pn, uint32_t base_n, uint32_t &err, uint32_t &perr,
+                                            int &ndis)
+{
+    using SM = ChunkSmem<Real, Acc, BT, PPT, CAP, STAGES>;
+    constexpr int CH = SM::CH;
+    constexpr int NW = BT / 32;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const typename SM::Stage &sg = sm.stage[s];
+    const int wbase = wid * 32 * PPT + lane;
+
+    // box of the chunk's enabled, in-range cells
+    unsigned xmn = 0xffffu, ymn = 0xffffu, xmx = 0, ymx = 0;
+    bool any = false;
+#pragma unroll
+    for (int j = 0; j < PPT; j++) {
+        const int local = wbase + 32 * j;
+        if (base + (uint32_t)local < (uint32_t)n) {
+            const uint2 key = sg.K[local];
+            const int cx = (int)(key.x & 0xffff), cy = (int)(key.x >> 16);
+            if (!(key.y & kDisabled) && cell_in_range(cx, cy, kp.gx, kp.gy)) {
+                xmn = min(xmn, (unsigned)cx); ymn = min(ymn, (unsigned)cy);
+                xmx = max(xmx, (unsigned)cx); ymx = max(ymx, (unsigned)cy);
+                any = true;
+            }
+        }
+    }
+    {
+        const unsigned FULL = 0xffffffffu;
+        xmn = __reduce_min_sync(FULL, xmn); ymn = __reduce_min_sync(FULL, ymn);
+        xmx = __reduce_max_sync(FULL, xmx); ymx = __reduce_max_sync(FULL, ymx);
+        const unsigned wany = __reduce_or_sync(FULL, any ? 1u : 0u);
+        if (lane == 0) {
+            sm.red[wid][0] = (int)xmn; sm.red[wid][1] = (int)ymn;
+            sm.red[wid][2] = (int)xmx; sm.red[wid][3] = (int)ymx; sm.red[wid][4] = (int)wany;
+        }
+    }
+    __syncthreads();
+    int bx0 = 0xffff, by0 = 0xffff, bx1 = 0, by1 = 0, bany = 0;
+#pragma unroll
+    for (int w = 0; w < NW; w++) {
+        bx0 = min(bx0, sm.red[w][0]); by0 = min(by0, sm.red[w][1]);
+        bx1 = max(bx1, sm.red[w][2]); by1 = max(by1, sm.red[w][3]); bany |= sm.red[w][4];
+    }
+    // scatter tile: cells +-2 (a point moves at most one cell per step)
+    Tile<Acc, CAP> T;
+    T.t = sm.tile;
+    T.x0 = bx0 - 2; T.y0 = by0 - 2;
+    T.tw = bx1 - bx0 + 5; T.th = by1 - by0 + 5;
+    // 64-bit products: a box spanning the whole grid must not wrap into range
+    T.on = bany && (long long)T.tw * (long long)T.th <= (long long)CAP;
+    if (!T.on) { T.tw = 0; T.th = 0; }
+    T.th_rcp = rcp32(T.th);
+    tile_zero<Acc, CAP, BT>(T);
+    __syncthreads();
+
+    Patch<Real> patch;
+    patch.have = false; patch.in_tile = false; patch.cx = patch.cy = 0;
+#pragma unroll 1
+    for (int j = 0; j < PPT; j++) {
+        const int local = wbase + 32 * j;
+        const uint32_t i = base + (uint32_t)local;
+        if (i >= (uint32_t)n) break;
+        const uint2 key = sg.K[local];
+        uint32_t util = key.y;
+        if (util & kDisabled) continue;
+        const V4<Real> A = sg.A[local];
+        const V4<Real> Hv = sg.H[local];
+        Real x = A.x, y = A.y, Jp = A.z;
+        const Real thick = A.w;
+        M2<Real> H = {Hv.x, Hv.y, Hv.z, Hv.w};
+        int cx = (int)(key.x & 0xffff), cy = (int)(key.x >> 16);
+        // forcing entry of the current cell, loaded early (points rarely change cell)
+        V4<Real> frc{};
+        if (kp.ext && cell_in_range(cx, cy, kp.gx, kp.gy)) frc = G.frc[(uint32_t)cx * (uint32_t)kp.gy + (uint32_t)cy];
+        Real vx = 0, vy = 0, c00 = 0, c01 = 0, c10 = 0, c11 = 0;
+        if (cell_in_range(cx, cy, kp.gx, kp.gy)) {
+            Real wx[3], wy[3];
+            bspline(x, wx);
+            bspline(y, wy);
+            V2<Real> nv[3][3];
+#pragma unroll
+            for (int a = 0; a < 3; a++) {
+                const uint32_t col = (uint32_t)(cx + a - 1) * (uint32_t)kp.gy + (uint32_t)(cy - 1);
+#pragma unroll
+                for (int b = 0; b < 3; b++) nv[a][b] = G.vel[col + b];
+            }
+            const Real gyv[3] = {wy[0] * (Real(-1) - y), wy[1] * (-y), wy[2] * (Real(1) - y)};
+            const Real gxv[3] = {wx[0] * (Real(-1) - x), wx[1] * (-x), wx[2] * (Real(1) - x)};
+            const Real ccx = nv[1][1].x, ccy = nv[1][1].y;
+            Real sx = 0, sy = 0, px = 0, py = 0, qx = 0, qy = 0;
+#pragma unroll
+            for (int a = 0; a < 3; a++) {
+                Real sax = 0, say = 0, tax = 0, tay = 0;
+#pragma unroll
+                for (int b = 0; b < 3; b++) {
+                    const Real dx = nv[a][b].x - ccx, dy = nv[a][b].y - ccy;
+                    sax += wy[b] * dx; say += wy[b] * dy;
+                    tax += gyv[b] * dx; tay += gyv[b] * dy;
+                }
+                sx += wx[a] * sax; sy += wx[a] * say;     // v_p - v_c
+                px += gxv[a] * sax; py += gxv[a] * say;   // x-derivative part
+                qx += wx[a] * tax; qy += wx[a] * tay;     // y-derivative part
+            }
+            vx = ccx + sx; vy = ccy + sy;
+            c00 = kp.four_h_inv * px; c10 = kp.four_h_inv * py;
+            c01 = kp.four_h_inv * qx; c11 = kp.four_h_inv * qy;
+        }
+        x += vx * kp.dt_h_inv;
+        y += vy * kp.dt_h_inv;
+        if (isnan(vx + vy)) err |= kErrVelNan;
+        if (isnan(x + y)) err |= kErrPosNan;
+        if (isnan((c00 + c10) + (c01 + c11))) err |= kErrBpNan;
+        bool moved = false;
+        if (x > Real(0.5)) { x -= Real(1); cx++; moved = true; }
+        else if (x < Real(-0.5)) { x += Real(1); cx--; moved = true; }
+        if (y > Real(0.5)) { y -= Real(1); cy++; moved = true; }
+        else if (y < Real(-0.5)) { y += Real(1); cy--; moved = true; }
+        if (moved && (cx <= 1 || cx >= kp.gx - 2 || cy <= 1 || cy >= kp.gy - 2)) {
+            util |= kDisabled;
+            ndis++;
+        }
+        if (x > Real(0.5) || x < Real(-0.5) || y > Real(0.5) || y < Real(-0.5)) err |= kErrJump;
+
+        // Fe <- (I + dt C) Fe, i.e. H <- H + D + D H with D = dt C
+        {
+            const Real d00 = kp.dt * c00, d01 = kp.dt * c01, d10 = kp.dt * c10, d11 = kp.dt * c11;
+            const M2<Real> h = H;
+            H.a00 = h.a00 + d00 + (d00 * h.a00 + d01 * h.a10);
+            H.a01 = h.a01 + d01 + (d00 * h.a01 + d01 * h.a11);
+            H.a10 = h.a10 + d10 + (d10 * h.a00 + d11 * h.a10);
+            H.a11 = h.a11 + d11 + (d10 * h.a01 + d11 * h.a11);
+        }
+        if (isnan((H.a00 + H.a10) + (H.a01 + H.a11))) err |= kErrFeNan;
+        Kin<Real> k = kinematics(H);
+        Real p_tr, q_tr;
+        pq(k, kp.mat.mu, kp.mat.kappa, p_tr, q_tr);
+        if (!(util & kCrushed)) util = failure_check(kp.mat, util, p_tr, q_tr);
+        if (util & kCrushed) {
+            const SvdH<Real> sv = svd_h(H);
+            wolper_dp(kp.mat, thick, p_tr, q_tr, k, sv, H, Jp);
+            if (isnan((H.a00 + H.a10) + (H.a01 + H.a11))) err |= kErrFeNan;
+            k = kinematics(H);
+        }
+
+        V4<Real> Ao; Ao.x = x; Ao.y = y; Ao.z = Jp; Ao.w = thick;
+        st_stream(P.A + i, Ao);
+        V4<Real> Ho; Ho.x = H.a00; Ho.y = H.a01; Ho.z = H.a10; Ho.w = H.a11;
+        st_stream(P.H + i, Ho);
+        if (store_vc || (util & kDisabled)) {   // a point disabled now keeps this step's V and C
+            V2<Real> Vo; Vo.x = vx; Vo.y = vy;
+            st_stream(P.V + i, Vo);
+            V4<Real> Co; Co.x = c00; Co.y = c01; Co.z = c10; Co.w = c11;
+            st_stream(P.C + i, Co);
+        }
+        const uint32_t cell = ((uint32_t)cy << 16) | (uint32_t)cx;   // as kernels.cuh:305
+        if (moved || util != key.y) {
+            uint2 ko; ko.x = moved ? cell : key.x; ko.y = util;
+            st_stream(P.K + i, ko);
+        }
+        if (recordPQ) { V2<Real> pqv; pqv.x = p_tr; pqv.y = q_tr; st_stream(P.PQ + i, pqv); }
+
+        if (!(util & kDisabled)) {
+            if (cell_in_range(cx, cy, kp.gx, kp.gy)) {
+                Src<Real> src;
+                src.cx = cx; src.cy = cy;
+                if (kp.ext && moved) frc = G.frc[(uint32_t)cx * (uint32_t)kp.gy + (uint32_t)cy];
+                make_src<Real, Acc>(kp, frc, src, x, y, Jp, thick, k, vx, vy, c00, c01, c10, c11, perr);
+                // NaN reaches these sums from any NaN term (the scatter's NaN checks)
+                const Real sw = (src.wx[0] + src.wx[1] + src.wx[2]) + (src.wy[0] + src.wy[1] + src.wy[2]);
+                if (isnan(sw + src.mp)) perr |= kErrP2gNanMass;
+                if (isnan(sw + ((src.ax + src.ay) + (src.s00 + src.s01) + (src.s10 + src.s11)))) perr |= kErrP2gNanVel;
+                patch_add<Real, Acc, CAP>(patch, src, T, G.acc, kp.gy);
+            } else {
+                perr |= kErrLeftArea;
+            }
+        }
+    }
+    // end patches: merge neighbours, then write into the tile.  For int64
+    // accumulators (whose shared atomics are multi-instruction sequences)
+    // the writes go without atomics in two phases (even warps, odd warps)
+    // when warps of one phase touch disjoint nodes and no warp has two
+    // lanes on one cell; float accumulators keep the native atomics.
+    if (!AccOps<Acc>::fixed) {
+        bool low = true, high = true;
+        patch_merge(patch, lane, low, high);
+        if (patch.have) {
+            if (patch.in_tile) patch_store<true, Real, Acc, CAP>(patch, T, true, low, high);
+            else patch_flush<Real, Acc, CAP>(patch, T, G.acc, kp.gy);
+        }
+        __syncthreads();
+    } else {
+        const unsigned FULL = 0xffffffffu;
+        bool low = true, high = true;
+        patch_merge(patch, lane, low, high);
+        if (patch.have && !patch.in_tile) patch_flush<Real, Acc, CAP>(patch, T, G.acc, kp.gy);
+        const bool mine = patch.have;
+        const uint32_t key = mine ? (((uint32_t)patch.cx << 16) | (uint32_t)patch.cy) : (0xffffffe0u | (uint32_t)lane);
+        // every lane takes part in the match (a lane skipped here would stall the warp)
+        const unsigned same = __match_any_sync(FULL, key);
+        const bool dup = __any_sync(FULL, mine && __popc(same) > 1);
+        const int x0 = __reduce_min_sync(FULL, mine ? patch.cx - 1 : INT_MAX);
+        const int x1 = __reduce_max_sync(FULL, mine ? patch.cx + 1 : INT_MIN);
+        const int y0 = __reduce_min_sync(FULL, mine ? patch.cy - 1 : INT_MAX);
+        const int y1 = __reduce_max_sync(FULL, mine ? patch.cy + 1 : INT_MIN);
+        if (lane == 0) {
+            sm.wbox[wid][0] = x0; sm.wbox[wid][1] = x1; sm.wbox[wid][2] = y0; sm.wbox[wid][3] = y1;
+            sm.wbox[wid][4] = dup ? 1 : 0;
+        }
+        __syncthreads();
+        bool phased = true;
+#pragma unroll
+        for (int w = 0; w < NW; w++) {
+            if (sm.wbox[w][4]) phased = false;
+#pragma unroll
+            for (int v = w + 2; v < NW; v += 2)
+                if (!(sm.wbox[w][1] < sm.wbox[v][0] || sm.wbox[v][1] < sm.wbox[w][0] ||
+                      sm.wbox[w][3] < sm.wbox[v][2] || sm.wbox[v][3] < sm.wbox[w][2]))
+                    phased = false;
+        }
+        if (phased) {
+            if ((wid & 1) == 0) patch_store<false, Real, Acc, CAP>(patch, T, mine, low, high);
+            __syncthreads();
+            if ((wid & 1) == 1) patch_store<false, Real, Acc, CAP>(patch, T, mine, low, high);
+        } else if (mine) {
+            patch_store<true, Real, Acc, CAP>(patch, T, true, low, high);
+        }
+        __syncthreads();
+    }
+    // one stage: its points are all read now, fetch the next chunk into it
+    if (STAGES == 1 && tid == 0 && next) fetch_chunk(sm.stage[0], Pn, base_n, CH, &sm.mbar[0]);
+    tile_flush<Acc, CAP, BT>(T, G.acc, kp.gx, kp.gy);
+}
+
 template <class Real, class Acc, int BT, int PPT, int CAP, int STAGES>
 __global__ void __launch_bounds__(BT, (sizeof(Real) == 8 ? 1 : ICEMPM_FUSED_MINB))
 k_g2p_p2g(KParams<Real> kp, Pts<Real> P, Grid<Real, Acc> G, DevStatus *st, int n, int nchunks)
@@ -756,10 +1010,9 @@ k_g2p_p2g(KParams<Real> kp, Pts<Real> P, Grid<Real, Acc> G, DevStatus *st, int n
     static_assert(STAGES == 1 || STAGES == 2, "one or two stages");
     using SM = ChunkSmem<Real, Acc, BT, PPT, CAP, STAGES>;
     constexpr int CH = SM::CH;
-    constexpr int NW = BT / 32;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     SM &sm = *reinterpret_cast<SM *>(smem_raw);
-    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const int tid = threadIdx.x;
 
     if (tid == 0) {
         mbar_init(&sm.mbar[0], 1);
@@ -781,234 +1034,11 @@ k_g2p_p2g(KParams<Real> kp, Pts<Real> P, Grid<Real, Acc> G, DevStatus *st, int n
         const uint32_t parity = STAGES == 2 ? ((uint32_t)(it >> 1) & 1u) : ((uint32_t)it & 1u);
         const bool ok = mbar_wait_bounded(&sm.mbar[s], parity);
         if (__syncthreads_or(!ok)) { err |= kErrBarrierTimeout; break; }
-        if (STAGES == 2 && tid == 0 && c + (int)gridDim.x < nchunks)
-            fetch_chunk(sm.stage[s ^ 1], P, (uint32_t)(c + (int)gridDim.x) * CH, CH, &sm.mbar[s ^ 1]);
-        const typename SM::Stage &sg = sm.stage[s];
-        const uint32_t base = (uint32_t)c * CH;
-        const int wbase = wid * 32 * PPT + lane;
-
-        // box of the chunk's enabled, in-range cells
-        unsigned xmn = 0xffffu, ymn = 0xffffu, xmx = 0, ymx = 0;
-        bool any = false;
-#pragma unroll
-        for (int j = 0; j < PPT; j++) {
-            const int local = wbase + 32 * j;
-            if (base + (uint32_t)local < (uint32_t)n) {
-                const uint2 key = sg.K[local];
-                const int cx = (int)(key.x & 0xffff), cy = (int)(key.x >> 16);
-                if (!(key.y & kDisabled) && cell_in_range(cx, cy, kp.gx, kp.gy)) {
-                    xmn = min(xmn, (unsigned)cx); ymn = min(ymn, (unsigned)cy);
-                    xmx = max(xmx, (unsigned)cx); ymx = max(ymx, (unsigned)cy);
-                    any = true;
-                }
-            }
-        }
-        {
-            const unsigned FULL = 0xffffffffu;
-            xmn = __reduce_min_sync(FULL, xmn); ymn = __reduce_min_sync(FULL, ymn);
-            xmx = __reduce_max_sync(FULL, xmx); ymx = __reduce_max_sync(FULL, ymx);
-            const unsigned wany = __reduce_or_sync(FULL, any ? 1u : 0u);
-            if (lane == 0) {
-                sm.red[wid][0] = (int)xmn; sm.red[wid][1] = (int)ymn;
-                sm.red[wid][2] = (int)xmx; sm.red[wid][3] = (int)ymx; sm.red[wid][4] = (int)wany;
-            }
-        }
-        __syncthreads();
-        int bx0 = 0xffff, by0 = 0xffff, bx1 = 0, by1 = 0, bany = 0;
-#pragma unroll
-        for (int w = 0; w < NW; w++) {
-            bx0 = min(bx0, sm.red[w][0]); by0 = min(by0, sm.red[w][1]);
-            bx1 = max(bx1, sm.red[w][2]); by1 = max(by1, sm.red[w][3]); bany |= sm.red[w][4];
-        }
-        // scatter tile: cells +-2 (a point moves at most one cell per step)
-        Tile<Acc, CAP> T;
-        T.t = sm.tile;
-        T.x0 = bx0 - 2; T.y0 = by0 - 2;
-        T.tw = bx1 - bx0 + 5; T.th = by1 - by0 + 5;
-        // 64-bit products: a box spanning the whole grid must not wrap into range
-        T.on = bany && (long long)T.tw * (long long)T.th <= (long long)CAP;
-        if (!T.on) { T.tw = 0; T.th = 0; }
-        T.th_rcp = rcp32(T.th);
-        tile_zero<Acc, CAP, BT>(T);
-        __syncthreads();
-
-        Patch<Real> patch;
-        patch.have = false; patch.in_tile = false; patch.cx = patch.cy = 0;
-#pragma unroll 1
-        for (int j = 0; j < PPT; j++) {
-            const int local = wbase + 32 * j;
-            const uint32_t i = base + (uint32_t)local;
-            if (i >= (uint32_t)n) break;
-            const uint2 key = sg.K[local];
-            uint32_t util = key.y;
-            if (util & kDisabled) continue;
-            const V4<Real> A = sg.A[local];
-            const V4<Real> Hv = sg.H[local];
-            Real x = A.x, y = A.y, Jp = A.z;
-            const Real thick = A.w;
-            M2<Real> H = {Hv.x, Hv.y, Hv.z, Hv.w};
-            int cx = (int)(key.x & 0xffff), cy = (int)(key.x >> 16);
-            // forcing entry of the current cell, loaded early (points rarely change cell)
-            V4<Real> frc{};
-            if (kp.ext && cell_in_range(cx, cy, kp.gx, kp.gy)) frc = G.frc[(uint32_t)cx * (uint32_t)kp.gy + (uint32_t)cy];
-            Real vx = 0, vy = 0, c00 = 0, c01 = 0, c10 = 0, c11 = 0;
-            if (cell_in_range(cx, cy, kp.gx, kp.gy)) {
-                Real wx[3], wy[3];
-                bspline(x, wx);
-                bspline(y, wy);
-                V2<Real> nv[3][3];
-#pragma unroll
-                for (int a = 0; a < 3; a++) {
-                    const uint32_t col = (uint32_t)(cx + a - 1) * (uint32_t)kp.gy + (uint32_t)(cy - 1);
-#pragma unroll
-                    for (int b = 0; b < 3; b++) nv[a][b] = G.vel[col + b];
-                }
-                const Real gyv[3] = {wy[0] * (Real(-1) - y), wy[1] * (-y), wy[2] * (Real(1) - y)};
-                const Real gxv[3] = {wx[0] * (Real(-1) - x), wx[1] * (-x), wx[2] * (Real(1) - x)};
-                const Real ccx = nv[1][1].x, ccy = nv[1][1].y;
-                Real sx = 0, sy = 0, px = 0, py = 0, qx = 0, qy = 0;
-#pragma unroll
-                for (int a = 0; a < 3; a++) {
-                    Real sax = 0, say = 0, tax = 0, tay = 0;
-#pragma unroll
-                    for (int b = 0; b < 3; b++) {
-                        const Real dx = nv[a][b].x - ccx, dy = nv[a][b].y - ccy;
-                        sax += wy[b] * dx; say += wy[b] * dy;
-                        tax += gyv[b] * dx; tay += gyv[b] * dy;
-                    }
-                    sx += wx[a] * sax; sy += wx[a] * say;     // v_p - v_c
-                    px += gxv[a] * sax; py += gxv[a] * say;   // x-derivative part
-                    qx += wx[a] * tax; qy += wx[a] * tay;     // y-derivative part
-                }
-                vx = ccx + sx; vy = ccy + sy;
-                c00 = kp.four_h_inv * px; c10 = kp.four_h_inv * py;
-                c01 = kp.four_h_inv * qx; c11 = kp.four_h_inv * qy;
-            }
-            x += vx * kp.dt_h_inv;
-            y += vy * kp.dt_h_inv;
-            if (isnan(vx + vy)) err |= kErrVelNan;
-            if (isnan(x + y)) err |= kErrPosNan;
-            if (isnan((c00 + c10) + (c01 + c11))) err |= kErrBpNan;
-            bool moved = false;
-            if (x > Real(0.5)) { x -= Real(1); cx++; moved = true; }
-            else if (x < Real(-0.5)) { x += Real(1); cx--; moved = true; }
-            if (y > Real(0.5)) { y -= Real(1); cy++; moved = true; }
-            else if (y < Real(-0.5)) { y += Real(1); cy--; moved = true; }
-            if (moved && (cx <= 1 || cx >= kp.gx - 2 || cy <= 1 || cy >= kp.gy - 2)) {
-                util |= kDisabled;
-                ndis++;
-            }
-            if (x > Real(0.5) || x < Real(-0.5) || y > Real(0.5) || y < Real(-0.5)) err |= kErrJump;
-
-            // Fe <- (I + dt C) Fe, i.e. H <- H + D + D H with D = dt C
-            {
-                const Real d00 = kp.dt * c00, d01 = kp.dt * c01, d10 = kp.dt * c10, d11 = kp.dt * c11;
-                const M2<Real> h = H;
-                H.a00 = h.a00 + d00 + (d00 * h.a00 + d01 * h.a10);
-                H.a01 = h.a01 + d01 + (d00 * h.a01 + d01 * h.a11);
-                H.a10 = h.a10 + d10 + (d10 * h.a00 + d11 * h.a10);
-                H.a11 = h.a11 + d11 + (d10 * h.a01 + d11 * h.a11);
-            }
-            if (isnan((H.a00 + H.a10) + (H.a01 + H.a11))) err |= kErrFeNan;
-            Kin<Real> k = kinematics(H);
-            Real p_tr, q_tr;
-            pq(k, kp.mat.mu, kp.mat.kappa, p_tr, q_tr);
-            if (!(util & kCrushed)) util = failure_check(kp.mat, util, p_tr, q_tr);
-            if (util & kCrushed) {
-                const SvdH<Real> sv = svd_h(H);
-                wolper_dp(kp.mat, thick, p_tr, q_tr, k, sv, H, Jp);
-                if (isnan((H.a00 + H.a10) + (H.a01 + H.a11))) err |= kErrFeNan;
-                k = kinematics(H);
-            }
-
-            V4<Real> Ao; Ao.x = x; Ao.y = y; Ao.z = Jp; Ao.w = thick;
-            st_stream(P.A + i, Ao);
-            V4<Real> Ho; Ho.x = H.a00; Ho.y = H.a01; Ho.z = H.a10; Ho.w = H.a11;
-            st_stream(P.H + i, Ho);
-            if (store_vc || (util & kDisabled)) {   // a point disabled now keeps this step's V and C
-                V2<Real> Vo; Vo.x = vx; Vo.y = vy;
-                st_stream(P.V + i, Vo);
-                V4<Real> Co; Co.x = c00; Co.y = c01; Co.z = c10; Co.w = c11;
-                st_stream(P.C + i, Co);
-            }
-            const uint32_t cell = ((uint32_t)cy << 16) | (uint32_t)cx;   // as kernels.cuh:305
-            if (moved || util != key.y) {
-                uint2 ko; ko.x = moved ? cell : key.x; ko.y = util;
-                st_stream(P.K + i, ko);
-            }
-            if (recordPQ) { V2<Real> pqv; pqv.x = p_tr; pqv.y = q_tr; st_stream(P.PQ + i, pqv); }
-
-            if (!(util & kDisabled)) {
-                if (cell_in_range(cx, cy, kp.gx, kp.gy)) {
-                    Src<Real> src;
-                    src.cx = cx; src.cy = cy;
-                    if (kp.ext && moved) frc = G.frc[(uint32_t)cx * (uint32_t)kp.gy + (uint32_t)cy];
-                    make_src<Real, Acc>(kp, frc, src, x, y, Jp, thick, k, vx, vy, c00, c01, c10, c11, perr);
-                    // NaN reaches these sums from any NaN term (the scatter's NaN checks)
-                    const Real sw = (src.wx[0] + src.wx[1] + src.wx[2]) + (src.wy[0] + src.wy[1] + src.wy[2]);
-                    if (isnan(sw + src.mp)) perr |= kErrP2gNanMass;
-                    if (isnan(sw + ((src.ax + src.ay) + (src.s00 + src.s01) + (src.s10 + src.s11)))) perr |= kErrP2gNanVel;
-                    patch_add<Real, Acc, CAP>(patch, src, T, G.acc, kp.gy);
-                } else {
-                    perr |= kErrLeftArea;
-                }
-            }
-        }
-        // end patches: merge neighbours, then write into the tile.  For int64
-        // accumulators (whose shared atomics are multi-instruction sequences)
-        // the writes go without atomics in two phases (even warps, odd warps)
-        // when warps of one phase touch disjoint nodes and no warp has two
-        // lanes on one cell; float accumulators keep the native atomics.
-        if (!AccOps<Acc>::fixed) {
-            bool low = true, high = true;
-            patch_merge(patch, lane, low, high);
-            if (patch.have) {
-                if (patch.in_tile) patch_store<true, Real, Acc, CAP>(patch, T, true, low, high);
-                else patch_flush<Real, Acc, CAP>(patch, T, G.acc, kp.gy);
-            }
-            __syncthreads();
-        } else {
-            const unsigned FULL = 0xffffffffu;
-            bool low = true, high = true;
-            patch_merge(patch, lane, low, high);
-            if (patch.have && !patch.in_tile) patch_flush<Real, Acc, CAP>(patch, T, G.acc, kp.gy);
-            const bool mine = patch.have;
-            const uint32_t key = mine ? (((uint32_t)patch.cx << 16) | (uint32_t)patch.cy) : (0xffffffe0u | (uint32_t)lane);
-            // every lane takes part in the match (a lane skipped here would stall the warp)
-            const unsigned same = __match_any_sync(FULL, key);
-            const bool dup = __any_sync(FULL, mine && __popc(same) > 1);
-            const int x0 = __reduce_min_sync(FULL, mine ? patch.cx - 1 : INT_MAX);
-            const int x1 = __reduce_max_sync(FULL, mine ? patch.cx + 1 : INT_MIN);
-            const int y0 = __reduce_min_sync(FULL, mine ? patch.cy - 1 : INT_MAX);
-            const int y1 = __reduce_max_sync(FULL, mine ? patch.cy + 1 : INT_MIN);
-            if (lane == 0) {
-                sm.wbox[wid][0] = x0; sm.wbox[wid][1] = x1; sm.wbox[wid][2] = y0; sm.wbox[wid][3] = y1;
-                sm.wbox[wid][4] = dup ? 1 : 0;
-            }
-            __syncthreads();
-            bool phased = true;
-#pragma unroll
-            for (int w = 0; w < NW; w++) {
-                if (sm.wbox[w][4]) phased = false;
-#pragma unroll
-                for (int v = w + 2; v < NW; v += 2)
-                    if (!(sm.wbox[w][1] < sm.wbox[v][0] || sm.wbox[v][1] < sm.wbox[w][0] ||
-                          sm.wbox[w][3] < sm.wbox[v][2] || sm.wbox[v][3] < sm.wbox[w][2]))
-                        phased = false;
-            }
-            if (phased) {
-                if ((wid & 1) == 0) patch_store<false, Real, Acc, CAP>(patch, T, mine, low, high);
-                __syncthreads();
-                if ((wid & 1) == 1) patch_store<false, Real, Acc, CAP>(patch, T, mine, low, high);
-            } else if (mine) {
-                patch_store<true, Real, Acc, CAP>(patch, T, true, low, high);
-            }
-            __syncthreads();
-        }
-        // one stage: its points are all read now, fetch the next chunk into it
-        if (STAGES == 1 && tid == 0 && c + (int)gridDim.x < nchunks)
-            fetch_chunk(sm.stage[0], P, (uint32_t)(c + (int)gridDim.x) * CH, CH, &sm.mbar[0]);
-        tile_flush<Acc, CAP, BT>(T, G.acc, kp.gx, kp.gy);
+        const bool next = c + (int)gridDim.x < nchunks;
+        const uint32_t base_n = (uint32_t)(c + (int)gridDim.x) * CH;
+        if (STAGES == 2 && tid == 0 && next) fetch_chunk(sm.stage[s ^ 1], P, base_n, CH, &sm.mbar[s ^ 1]);
+        fused_chunk<Real, Acc, BT, PPT, CAP, STAGES>(sm, s, kp, P, G, (uint32_t)c * CH, n, recordPQ, store_vc, next, P,
+                                                     base_n, err, perr, ndis);
     }
     warp_flush_status(st, err, perr, ndis);
 
@@ -1020,6 +1050,97 @@ k_g2p_p2g(KParams<Real> kp, Pts<Real> P, Grid<Real, Acc> G, DevStatus *st, int n
         if (t == gridDim.x - 1) {
             st->step = step + 1;
             st->done = 0;
+            __threadfence();
+        }
+    }
+}
+
+// ---- ensembles: many independent scenes in one launch ------------------------
+// Each scene is an ordinary context (its own points, grid, parameters and
+// status); a table of their descriptors lets one launch of each kernel walk
+// the chunks (fused kernel) and nodes (grid update) of all of them.  The
+// batch's own DevStatus carries the common sub-step counter.
+template <class Real, class Acc> struct SceneDesc {
+    KParams<Real> kp;
+    Pts<Real> P;
+    Grid<Real, Acc> G;
+    DevStatus *st;
+    int n;             // entries of the point arrays (points + placeholders)
+    int chunk0;        // first global chunk of this scene
+    long long nnodes;
+    int block0;        // first global 256-node block of this scene
+    int ext;           // extended forcing
+};
+
+template <class Real, class Acc>
+__global__ void __launch_bounds__(256) k_grid_update_batch(const SceneDesc<Real, Acc> *__restrict__ scenes,
+                                                           const int *__restrict__ block_scene, DevStatus *bst)
+{
+    const int si = block_scene[blockIdx.x];
+    const SceneDesc<Real, Acc> &S = scenes[si];
+    const long long idx = (long long)(blockIdx.x - S.block0) * 256 + threadIdx.x;
+    if (idx == 0) fold_pending(S.st);
+    if (idx >= S.nnodes) return;
+    if (S.ext) grid_update_node<Real, Acc, true>(S.kp, S.G, S.st, idx, bst->step);
+    else grid_update_node<Real, Acc, false>(S.kp, S.G, S.st, idx, bst->step);
+}
+
+template <class Real, class Acc, int BT, int PPT, int CAP, int STAGES>
+__global__ void __launch_bounds__(BT, (sizeof(Real) == 8 ? 1 : ICEMPM_FUSED_MINB))
+k_g2p_p2g_batch(const SceneDesc<Real, Acc> *__restrict__ scenes, const int *__restrict__ chunk_scene, int nchunks,
+                DevStatus *bst)
+{
+    static_assert(STAGES == 1 || STAGES == 2, "one or two stages");
+    using SM = ChunkSmem<Real, Acc, BT, PPT, CAP, STAGES>;
+    constexpr int CH = SM::CH;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    SM &sm = *reinterpret_cast<SM *>(smem_raw);
+    const int tid = threadIdx.x;
+
+    if (tid == 0) {
+        mbar_init(&sm.mbar[0], 1);
+        if (STAGES == 2) mbar_init(&sm.mbar[1], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    int c = blockIdx.x;
+    if (tid == 0 && c < nchunks) {
+        const SceneDesc<Real, Acc> &S0 = scenes[chunk_scene[c]];
+        fetch_chunk(sm.stage[0], S0.P, (uint32_t)(c - S0.chunk0) * CH, CH, &sm.mbar[0]);
+    }
+    const int step = bst->step;
+    const bool store_vc = step == bst->vc_step;
+
+    for (int it = 0; c < nchunks; it++, c += (int)gridDim.x) {
+        const SceneDesc<Real, Acc> &S = scenes[chunk_scene[c]];
+        const int s = STAGES == 2 ? (it & 1) : 0;
+        const uint32_t parity = STAGES == 2 ? ((uint32_t)(it >> 1) & 1u) : ((uint32_t)it & 1u);
+        uint32_t err = 0, perr = 0;
+        int ndis = 0;
+        const bool ok = mbar_wait_bounded(&sm.mbar[s], parity);
+        if (__syncthreads_or(!ok)) {
+            warp_flush_status(S.st, kErrBarrierTimeout, 0u, 0);
+            break;
+        }
+        const int cn = c + (int)gridDim.x;
+        const bool next = cn < nchunks;
+        const SceneDesc<Real, Acc> &Sn = scenes[chunk_scene[next ? cn : c]];
+        const uint32_t base_n = (uint32_t)(cn - Sn.chunk0) * CH;
+        if (STAGES == 2 && tid == 0 && next) fetch_chunk(sm.stage[s ^ 1], Sn.P, base_n, CH, &sm.mbar[s ^ 1]);
+        const bool recordPQ = S.kp.update_every > 0 && (step % S.kp.update_every) == 0;
+        fused_chunk<Real, Acc, BT, PPT, CAP, STAGES>(sm, s, S.kp, S.P, S.G, (uint32_t)(c - S.chunk0) * CH, S.n,
+                                                     recordPQ, store_vc, next, Sn.P, base_n, err, perr, ndis);
+        warp_flush_status(S.st, err, perr, ndis);
+    }
+
+    // the last CTA to finish advances the batch's sub-step counter
+    __syncthreads();
+    if (tid == 0) {
+        __threadfence();
+        const unsigned t = atomicAdd(&bst->done, 1u);
+        if (t == gridDim.x - 1) {
+            bst->step = step + 1;
+            bst->done = 0;
             __threadfence();
         }
     }

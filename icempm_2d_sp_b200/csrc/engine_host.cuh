@@ -22,8 +22,13 @@ namespace icempm {
 
 static inline double pow2_floor(double x) { return std::ldexp(1.0, (int)std::floor(std::log2(x))); }
 
+template <class Real, class Acc> class BatchT;
+
 template <class Real, class Acc>
 class EngineT final : public Engine {
+    friend class BatchT<Real, Acc>;
+
+public:
     // fused kernel: threads per CTA and points per thread (a chunk of BT*PPT
     // points per CTA iteration; FP64 state halves the chunk to fit two stages)
     static constexpr int BT = sizeof(Real) == 8 ? 128 : ICEMPM_FUSED_BT;
@@ -36,7 +41,6 @@ class EngineT final : public Engine {
     static constexpr int STAGES = ICEMPM_FUSED_STAGES;
     using FusedSmem = ChunkSmem<Real, Acc, BT, PPT, CAP, STAGES>;
 
-public:
     EngineT() = default;
     ~EngineT() override { release(); }
 
@@ -550,6 +554,7 @@ public:
     }
 
     uint32_t count() const override { return n_real_; }
+    int device() const { return opts_.device; }
     cudaStream_t stream() const override { return stream_; }
     uint64_t launches() const override { return launches_; }
     double fixed_scale_m() const override { return kp_.scale_m; }

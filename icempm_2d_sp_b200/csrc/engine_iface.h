@@ -35,8 +35,24 @@ public:
     virtual double fixed_scale_p() const = 0;
 };
 
+// Ensemble of contexts of one variant stepped together (batch.cuh).
+class Batch {
+public:
+    virtual ~Batch() {}
+    virtual int step(int nsteps, int first_step) = 0;
+    virtual int timings(float ms[4]) = 0;
+    virtual int autotune(int trial_steps, int first_step, icempm_batch_tuning_t *out) = 0;
+    virtual int set_tuning(const icempm_batch_tuning_t *t) = 0;
+    virtual int get_tuning(icempm_batch_tuning_t *t) const = 0;
+    virtual uint64_t launches() const = 0;
+};
+
 Engine *make_engine_fixed();
 Engine *make_engine_fp32();
 Engine *make_engine_fp64();
+// nullptr (with the message recorded) when the contexts do not fit one batch
+Batch *make_batch_fixed(Engine *const *engines, int count);
+Batch *make_batch_fp32(Engine *const *engines, int count);
+Batch *make_batch_fp64(Engine *const *engines, int count);
 
 }  // namespace icempm

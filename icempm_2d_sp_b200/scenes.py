@@ -174,6 +174,8 @@ def config1(seed=1235, gx=4096, gy=2048, n_seeds=2000, keep=0.7, forcing=FORCING
         order = rng.permutation(len(ids))
         csum = np.cumsum(counts[order] * 4)
         keep_ids = ids[order][csum <= max_points]
+        if len(keep_ids) == 0 and len(ids):   # every floe is larger than the cap: keep the smallest
+            keep_ids = ids[np.argmin(counts)][None]
         floe = np.where(np.isin(floe, keep_ids), floe, -1)
     ice = floe >= 0
     x, y, k = lattice_points(cx[ice], cy[ice], h, rng)
@@ -189,6 +191,50 @@ def config1(seed=1235, gx=4096, gy=2048, n_seeds=2000, keep=0.7, forcing=FORCING
     return Scene("config1", p, wall_ring_status(gx, gy), uniform_current(gx, gy, 0.1),
                  soa, len(x), 200, opts, seed,
                  info={"floes_kept": int(len(np.unique(floe[ice]))), "n_seeds": n_seeds})
+
+
+# grid sizes an ensemble scene picks from (cells, smallest that fits its points)
+ENSEMBLE_GRIDS = [(128, 128), (256, 128), (256, 256), (512, 256), (512, 512), (1024, 512), (1024, 1024),
+                  (2048, 1024)]
+
+
+def ensemble_scene(seed, target_points, wind_speed, wind_dir, current_speed, current_dir,
+                   forcing=FORCING_EXTENDED) -> Scene:
+    """One scene of the batched-ensemble workload: config-1 generation rules
+    (Voronoi floes, 70% kept, 4 ppc, lognormal thickness) on the smallest grid
+    of ENSEMBLE_GRIDS that holds `target_points`, whole floes kept up to that
+    count; uniform wind and current of the given speeds and directions."""
+    gx, gy = ENSEMBLE_GRIDS[-1]
+    for g in ENSEMBLE_GRIDS:
+        if g[0] * g[1] * 4 * 0.7 * 0.8 >= target_points:
+            gx, gy = g
+            break
+    n_seeds = max(8, round(gx * gy / 1500))   # floes of ~1500 cells, so whole floes approach the target
+    sc = config1(seed=seed, gx=gx, gy=gy, n_seeds=n_seeds, forcing=forcing, max_points=target_points)
+    sc.options.wind_kind = WIND_UNIFORM
+    sc.options.wind_u = float(wind_speed * np.cos(wind_dir))
+    sc.options.wind_v = float(wind_speed * np.sin(wind_dir))
+    sc.current = uniform_current(gx, gy, float(current_speed * np.cos(current_dir)),
+                                 float(current_speed * np.sin(current_dir)))
+    sc.name = "ensemble"
+    sc.info.update({"target_points": int(target_points), "wind_speed": float(wind_speed),
+                    "current_speed": float(current_speed)})
+    return sc
+
+
+def ensemble(n_scenes=96, seed=4242, n_min=10_000, n_max=2_000_000, forcing=FORCING_EXTENDED):
+    """Batched-ensemble workload: `n_scenes` independent
+    scenes, point counts log-uniform in [n_min, n_max], Voronoi floes as in
+    config 1, grids from 128x128 to 2048x1024 sized to each scene, wind speed
+    uniform in 5-25 m/s with a uniform direction, current uniform in
+    0-0.3 m/s with a uniform direction."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n_scenes):
+        target = int(np.exp(rng.uniform(np.log(n_min), np.log(n_max))))
+        out.append(ensemble_scene(seed + 1 + k, target, rng.uniform(5.0, 25.0), rng.uniform(0, 2 * np.pi),
+                                  rng.uniform(0.0, 0.3), rng.uniform(0, 2 * np.pi), forcing=forcing))
+    return out
 
 
 def ridging(seed=1236, gx=1024, gy=512, cells_x=500, cells_y=500, h=2.0, dt=2e-4,

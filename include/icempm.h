@@ -283,6 +283,40 @@ ICEMPM_API int icempm_launch_count(icempm_t *ctx, uint64_t *count);
 ICEMPM_API int icempm_cell_order_noalloc(const uint32_t *d_cell, const uint32_t *d_utility, uint32_t n,
                                          int32_t grid_y, uint32_t *d_order, uint32_t *d_count, void *stream);
 
+/* ---- Ensembles (no counterpart in the reference) --------
+ * Many independent scenes advanced together: one launch of the grid update
+ * and one of the fused kernel per sub-step cover every scene of the batch,
+ * captured in CUDA graphs.  Each scene is an ordinary context (created,
+ * uploaded, downloaded, queried, sorted and compacted through the calls
+ * above); all contexts of a batch share the variant and the device and must
+ * outlive the batch.  The batch advances all scenes in lockstep: sub-step
+ * index first_step .. first_step+nsteps-1 for each, at each scene's own dt. */
+typedef struct icempm_batch icempm_batch_t;
+
+typedef struct icempm_batch_tuning_t {
+    int32_t tile_nodes;    /* shared scatter tile of the fused kernel: 512 or 1024 nodes */
+    int32_t stages;        /* bulk-copy stages of point state: 1 or 2 (512 nodes only) */
+    int32_t sort_every;    /* locality sort of every scene each this many sub-steps; 0 = never */
+    int32_t graph_steps;   /* sub-steps per CUDA graph; 0 = direct launches */
+    float ms_per_step;     /* set by icempm_batch_autotune: the chosen form's time per sub-step */
+    int32_t reserved[3];
+} icempm_batch_tuning_t;
+
+ICEMPM_API int icempm_batch_create(icempm_t *const *contexts, int32_t count, icempm_batch_t **out);
+ICEMPM_API int icempm_batch_destroy(icempm_batch_t *batch);
+/* Blocks until the sub-steps are done (the contexts' own calls may follow). */
+ICEMPM_API int icempm_batch_step(icempm_batch_t *batch, int32_t nsteps, int32_t first_step);
+/* Project autotuner: times the kernel shapes and sort cadences on the live
+ * scenes (which advance by 4 * trial_steps sub-steps, indices from first_step)
+ * and keeps the fastest; the choice is returned in *out (may be NULL). */
+ICEMPM_API int icempm_batch_autotune(icempm_batch_t *batch, int32_t trial_steps, int32_t first_step,
+                                     icempm_batch_tuning_t *out);
+ICEMPM_API int icempm_batch_set_tuning(icempm_batch_t *batch, const icempm_batch_tuning_t *tuning);
+ICEMPM_API int icempm_batch_get_tuning(icempm_batch_t *batch, icempm_batch_tuning_t *tuning);
+/* ms[0] = device time of the last icempm_batch_step; ms[1..3] = 0. */
+ICEMPM_API int icempm_batch_timings(icempm_batch_t *batch, float ms[4]);
+ICEMPM_API int icempm_batch_launch_count(icempm_batch_t *batch, uint64_t *count);
+
 /* Message of the last failing call on this thread ("" if none). */
 ICEMPM_API const char *icempm_last_error(void);
 

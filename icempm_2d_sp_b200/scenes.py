@@ -228,13 +228,33 @@ def ensemble(n_scenes=96, seed=4242, n_min=10_000, n_max=2_000_000, forcing=FORC
     config 1, grids from 128x128 to 2048x1024 sized to each scene, wind speed
     uniform in 5-25 m/s with a uniform direction, current uniform in
     0-0.3 m/s with a uniform direction."""
+    return [ensemble_scene(**spec, forcing=forcing) for spec in ensemble_specs(n_scenes, seed, n_min, n_max)]
+
+
+def ensemble_specs(n_scenes=96, seed=4242, n_min=10_000, n_max=2_000_000):
+    """The draws behind ensemble(): one dict of ensemble_scene arguments per
+    scene, cheap to compute, so that ranks can split the scenes by size before
+    generating only their own."""
     rng = np.random.default_rng(seed)
     out = []
     for k in range(n_scenes):
         target = int(np.exp(rng.uniform(np.log(n_min), np.log(n_max))))
-        out.append(ensemble_scene(seed + 1 + k, target, rng.uniform(5.0, 25.0), rng.uniform(0, 2 * np.pi),
-                                  rng.uniform(0.0, 0.3), rng.uniform(0, 2 * np.pi), forcing=forcing))
+        out.append(dict(seed=seed + 1 + k, target_points=target, wind_speed=rng.uniform(5.0, 25.0),
+                        wind_dir=rng.uniform(0, 2 * np.pi), current_speed=rng.uniform(0.0, 0.3),
+                        current_dir=rng.uniform(0, 2 * np.pi)))
     return out
+
+
+def split_by_size(sizes, parts):
+    """Scene indices for each of `parts` ranks, largest scenes first onto the
+    least-loaded rank, so each rank's point total is about the same."""
+    load = [0] * parts
+    out = [[] for _ in range(parts)]
+    for i in sorted(range(len(sizes)), key=lambda i: -sizes[i]):
+        r = min(range(parts), key=lambda r: load[r])
+        out[r].append(i)
+        load[r] += sizes[i]
+    return [sorted(o) for o in out]
 
 
 def ridging(seed=1236, gx=1024, gy=512, cells_x=500, cells_y=500, h=2.0, dt=2e-4,

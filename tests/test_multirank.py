@@ -70,3 +70,16 @@ def test_reference_arm_under_torchrun_prints_once(tmp_path):
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["cpu_baseline"]["kind"] in ("reference", "port")
+
+
+def test_ensemble_scenes_split_by_size_over_ranks():
+    """bench.py --workload ensemble under torchrun: each rank generates and
+    steps its share of the scenes; every scene goes to exactly one rank and
+    the ranks' point totals stay within a few percent of each other."""
+    from icempm_2d_sp_b200 import scenes
+    sizes = [s["target_points"] for s in scenes.ensemble_specs(96)]
+    for world in (1, 2, 4, 8):
+        parts = scenes.split_by_size(sizes, world)
+        assert sorted(i for p in parts for i in p) == list(range(96))
+        loads = [sum(sizes[i] for i in p) for p in parts]
+        assert max(loads) <= 1.05 * min(loads)

@@ -22,7 +22,7 @@ FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fvisibility=hid
          "--expt-relaxed-constexpr", "-I", os.path.join(ROOT, "include")]
 # developer knob for tuning builds, e.g. ICEMPM_EXTRA_FLAGS="-maxrregcount=96"
 FLAGS += os.environ.get("ICEMPM_EXTRA_FLAGS", "").split()
-SOURCES = ["capi.cu", "engine_fixed.cu", "engine_fp32.cu", "engine_fp64.cu", "noalloc.cu"]
+SOURCES = ["capi.cu", "engine_fixed.cu", "engine_fp32.cu", "engine_fp64.cu", "noalloc.cu", "surrogate.cu"]
 # The FP32-state engines use approximate single-precision division and square
 # root (a few ulp, far inside the parity tolerances); the FP64 engine is exact.
 PER_SOURCE = {"engine_fixed.cu": ["-use_fast_math"], "engine_fp32.cu": ["-use_fast_math"]}

@@ -22,6 +22,8 @@ EXPORTS = [
     "icempm_get_stream", "icempm_launch_count", "icempm_last_error", "icempm_cell_order_noalloc",
     "icempm_batch_create", "icempm_batch_destroy", "icempm_batch_step", "icempm_batch_autotune",
     "icempm_batch_set_tuning", "icempm_batch_get_tuning", "icempm_batch_timings", "icempm_batch_launch_count",
+    "icempm_mlp_param_count", "icempm_mlp_grad", "icempm_mlp_adam", "icempm_mlp_forward", "icempm_return_map_exact",
+    "icempm_return_map_learned", "icempm_harvest_begin", "icempm_harvest_end",
 ]
 
 
@@ -88,6 +90,17 @@ def load(path: str = LIB_PATH):
         "icempm_batch_get_tuning": (C.c_int, [h, C.POINTER(BatchTuning)]),
         "icempm_batch_timings": (C.c_int, [h, C.POINTER(C.c_float)]),
         "icempm_batch_launch_count": (C.c_int, [h, C.POINTER(C.c_uint64)]),
+        "icempm_mlp_param_count": (C.c_int, []),
+        "icempm_mlp_grad": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p,
+                                      C.c_void_p]),
+        "icempm_mlp_adam": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_float,
+                                      C.c_void_p]),
+        "icempm_mlp_forward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
+        "icempm_return_map_exact": (C.c_int, [sp, C.c_void_p, C.c_uint32, C.c_void_p, C.c_int32, C.c_void_p]),
+        "icempm_return_map_learned": (C.c_int, [sp, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_float,
+                                                C.c_void_p, C.c_void_p, C.c_void_p]),
+        "icempm_harvest_begin": (C.c_int, [h, C.c_uint32, C.c_int32]),
+        "icempm_harvest_end": (C.c_int, [h, C.POINTER(C.c_float), C.c_uint32, C.POINTER(C.c_uint32)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -127,6 +140,19 @@ def host_unregister(arr: np.ndarray) -> None:
 
 class Context:
     """One scene on one GPU behind the C ABI (the role of GPU_Implementation5)."""
+
+    def harvest_begin(self, capacity, stride=1):
+        """Record return-map projections of the following steps (icempm_harvest_begin)."""
+        check(self._L.icempm_harvest_begin(self.h, int(capacity), int(stride)))
+        self._harvest_cap = int(capacity)
+
+    def harvest_end(self):
+        """The recorded (trial, projected) pairs as float32 [count, 8], and how many were offered."""
+        cap = self._harvest_cap
+        rec = np.zeros((cap, 8), np.float32)
+        cnt = C.c_uint32(0)
+        check(self._L.icempm_harvest_end(self.h, rec.ctypes.data_as(C.POINTER(C.c_float)), cap, C.byref(cnt)))
+        return rec[:min(cnt.value, cap)], cnt.value
 
     def __init__(self, prms: SimParams, grid_status: np.ndarray, current=None, capacity: int = 0,
                  options: Options = None):

@@ -242,6 +242,18 @@ int icempm_device_count(int *count)
     return ICEMPM_OK;
 }
 
+int icempm_harvest_begin(icempm_t *ctx, uint32_t capacity, int32_t stride)
+{
+    ICEMPM_GUARD_CTX(ctx);
+    ICEMPM_TRY(ctx->eng->harvest_begin(capacity, stride));
+}
+
+int icempm_harvest_end(icempm_t *ctx, float *records, uint32_t capacity, uint32_t *count)
+{
+    ICEMPM_GUARD_CTX(ctx);
+    ICEMPM_TRY(ctx->eng->harvest_end(records, capacity, count));
+}
+
 int icempm_batch_create(icempm_t *const *contexts, int32_t count, icempm_batch_t **out)
 {
     if (!out) return fail(ICEMPM_E_ARG, "out is null");

@@ -32,6 +32,7 @@
 //   vel {vx, vy}                   grid velocity after the update
 //   status (u8), cur {vx, vy}, force {fx, fy} (f64, boundary reaction)
 #pragma once
+#include <cmath>
 #include <cstdint>
 #include <cstring>
 #include <climits>
@@ -141,6 +142,31 @@ template <class Real, class Acc> struct Grid {
     double2 *force;
 };
 
+// The yield-surface and hardening constants of SimParams
+// (GetParametersForGrain, kernels.cuh:538-566; tan is taken once here).
+inline Material material_of(const icempm_simparams_t &p)
+{
+    Material m;
+    m.mu = p.mu; m.kappa = p.kappa; m.DP_threshold_p = p.DP_threshold_p;
+    m.pmax = p.IceCompressiveStrength; m.pmin = -p.IceTensileStrength;
+    m.qmax = p.IceShearStrength; m.pmin2 = -p.IceTensileStrength2;
+    m.beta = p.IceTensileStrength / p.IceCompressiveStrength;
+    m.M_sq = (4. * m.qmax * m.qmax * (1. + 2. * m.beta)) / ((m.pmax - m.pmin) * (m.pmax - m.pmin));
+    m.tan_phi = std::tan(p.DP_phi * ICEMPM_PI / 180);
+    m.ridge_coeff_g_rho = p.RidgeFormationCoeff * ICEMPM_GRAVITY * p.IceDensity;
+    return m;
+}
+
+// Trial/projected pairs of the return map recorded from a run (training data
+// of the learned return map).  Record r is rec[2r] = {sigma1, sigma2, Jp_inv,
+// thickness} of the trial state and rec[2r+1] = {sigma1', sigma2', Jp_inv', 3}
+// after the projection; only projections onto the yield surface (case 3 of
+// the return map) are recorded.
+struct HarvestBuf {
+    uint32_t count, cap;
+    float4 *rec;
+};
+
 // Values the kernels read, prepared on the host from SimParams and the options.
 template <class Real> struct KParams {
     int gx, gy, update_every;
@@ -154,6 +180,8 @@ template <class Real> struct KParams {
     Real ext_impulse;               // dt * ParticleVolume (extended forcing)
     Real rho_w_cd;                  // rho_w * Cd (extended forcing)
     MatT<Real> mat;
+    HarvestBuf *harvest;            // return-map pairs are recorded when not null
+    int harvest_stride;             // ... for points with (index + step) % stride == 0
 };
 
 // Fire-and-forget reductions into global memory (red.global: no value comes
@@ -761,6 +789,25 @@ __device__ __forceinline__ void fetch_chunk(Stage &sg, const Pts<Real> &P, uint3
 // accumulators.  Every point of a chunk is read and written by the same
 // thread, so a stage can be refilled as soon as the CTA has passed the
 // barrier after its points.
+// Records one projection onto the yield surface (case 3 of wolper_dp) for the
+// learned return map: the trial singular values (sv), Jp_inv before (jp0) and
+// after, and the singular values of the projected state (H).
+template <class Real>
+__device__ __noinline__ void harvest_record(HarvestBuf *hb, const MatT<Real> &m, const SvdH<Real> &sv, Real p_tr,
+                                            Real q_tr, Real jp0, Real thick, const M2<Real> &H, Real jp1)
+{
+    if (p_tr < m.thr) return;                                   // cases 0/1: tension
+    const Real q_fs = p_tr < m.pmax ? m.fs_c * tsqrt((m.pmax - p_tr) * (p_tr - m.pmin)) : Real(0);
+    const Real q_dp = fmax(Real(0), (p_tr - m.thr) * m.tan_phi);
+    const Real q_yield = p_tr < m.pmax ? fmin(q_fs, q_dp) : Real(0);
+    if (!(q_tr > q_yield)) return;                              // case 2: elastic
+    const uint32_t r = atomicAdd(&hb->count, 1u);
+    if (r >= hb->cap) return;
+    const SvdH<Real> s1 = svd_h(H);
+    hb->rec[2 * (size_t)r] = make_float4(float(Real(1) + sv.e0), float(Real(1) + sv.e1), float(jp0), float(thick));
+    hb->rec[2 * (size_t)r + 1] = make_float4(float(Real(1) + s1.e0), float(Real(1) + s1.e1), float(jp1), 3.0f);
+}
+
 // One chunk of the fused kernel: CH = BT*PPT entries starting at `base` of a
 // scene's arrays, whose A, H, K are in stage `s`.  With one stage, the next
 // chunk (`next`, arrays Pn from base_n) is fetched into it once its points
@@ -769,7 +816,7 @@ __device__ __forceinline__ void fetch_chunk(Stage &sg, const Pts<Real> &P, uint3
 template <class Real, class Acc, int BT, int PPT, int CAP, int STAGES>
 __device__ __forceinline__ void fused_chunk(ChunkSmem<Real, Acc, BT, PPT, CAP, STAGES> &sm, int s,
                                             const KParams<Real> &kp, const Pts<Real> &P, const Grid<Real, Acc> &G,
-                                            uint32_t base, int n, bool recordPQ, bool store_vc, bool next,
+                                            uint32_t base, int n, int step, bool recordPQ, bool store_vc, bool next,
                                             const Pts<Real> &Pn, uint32_t base_n, uint32_t &err, uint32_t &perr,
                                             int &ndis)
 {
@@ -909,7 +956,10 @@ __device__ __forceinline__ void fused_chunk(ChunkSmem<Real, Acc, BT, PPT, CAP, S
         if (!(util & kCrushed)) util = failure_check(kp.mat, util, p_tr, q_tr);
         if (util & kCrushed) {
             const SvdH<Real> sv = svd_h(H);
+            const Real jp0 = Jp;
             wolper_dp(kp.mat, thick, p_tr, q_tr, k, sv, H, Jp);
+            if (kp.harvest && (i + (uint32_t)step) % (uint32_t)kp.harvest_stride == 0u)
+                harvest_record(kp.harvest, kp.mat, sv, p_tr, q_tr, jp0, thick, H, Jp);
             if (isnan((H.a00 + H.a10) + (H.a01 + H.a11))) err |= kErrFeNan;
             k = kinematics(H);
         }
@@ -1037,8 +1087,8 @@ k_g2p_p2g(KParams<Real> kp, Pts<Real> P, Grid<Real, Acc> G, DevStatus *st, int n
         const bool next = c + (int)gridDim.x < nchunks;
         const uint32_t base_n = (uint32_t)(c + (int)gridDim.x) * CH;
         if (STAGES == 2 && tid == 0 && next) fetch_chunk(sm.stage[s ^ 1], P, base_n, CH, &sm.mbar[s ^ 1]);
-        fused_chunk<Real, Acc, BT, PPT, CAP, STAGES>(sm, s, kp, P, G, (uint32_t)c * CH, n, recordPQ, store_vc, next, P,
-                                                     base_n, err, perr, ndis);
+        fused_chunk<Real, Acc, BT, PPT, CAP, STAGES>(sm, s, kp, P, G, (uint32_t)c * CH, n, step, recordPQ, store_vc,
+                                                     next, P, base_n, err, perr, ndis);
     }
     warp_flush_status(st, err, perr, ndis);
 
@@ -1128,7 +1178,7 @@ k_g2p_p2g_batch(const SceneDesc<Real, Acc> *__restrict__ scenes, const int *__re
         const uint32_t base_n = (uint32_t)(cn - Sn.chunk0) * CH;
         if (STAGES == 2 && tid == 0 && next) fetch_chunk(sm.stage[s ^ 1], Sn.P, base_n, CH, &sm.mbar[s ^ 1]);
         const bool recordPQ = S.kp.update_every > 0 && (step % S.kp.update_every) == 0;
-        fused_chunk<Real, Acc, BT, PPT, CAP, STAGES>(sm, s, S.kp, S.P, S.G, (uint32_t)(c - S.chunk0) * CH, S.n,
+        fused_chunk<Real, Acc, BT, PPT, CAP, STAGES>(sm, s, S.kp, S.P, S.G, (uint32_t)(c - S.chunk0) * CH, S.n, step,
                                                      recordPQ, store_vc, next, Sn.P, base_n, err, perr, ndis);
         warp_flush_status(S.st, err, perr, ndis);
     }

@@ -156,15 +156,10 @@ public:
         k.lim_p = (float)(std::ldexp(1.0, 56) / k.scale_p);
         k.ext_impulse = Real(p.InitialTimeStep * p.ParticleVolume);
         k.rho_w_cd = Real(opts_.water_density * opts_.water_drag_coeff);
-        Material m;
-        m.mu = p.mu; m.kappa = p.kappa; m.DP_threshold_p = p.DP_threshold_p;
-        m.pmax = p.IceCompressiveStrength; m.pmin = -p.IceTensileStrength;
-        m.qmax = p.IceShearStrength; m.pmin2 = -p.IceTensileStrength2;
-        m.beta = p.IceTensileStrength / p.IceCompressiveStrength;
-        m.M_sq = (4. * m.qmax * m.qmax * (1. + 2. * m.beta)) / ((m.pmax - m.pmin) * (m.pmax - m.pmin));
-        m.tan_phi = std::tan(p.DP_phi * ICEMPM_PI / 180);
-        m.ridge_coeff_g_rho = p.RidgeFormationCoeff * ICEMPM_GRAVITY * p.IceDensity;
+        const Material m = material_of(p);
         k.mat = mat_of<Real>(m);
+        k.harvest = harvest_;
+        k.harvest_stride = harvest_stride_;
         primed_ = false;
         invalidate_graphs();
         return 0;
@@ -553,6 +548,40 @@ public:
         return locality_sort();
     }
 
+    // Return-map pairs of the following steps (see HarvestBuf), at most
+    // `capacity` records, points with (index + step) % stride == 0.
+    int harvest_begin(uint32_t capacity, int stride) override
+    {
+        if (capacity == 0 || stride < 1) return fail(ICEMPM_E_ARG, "capacity must be > 0 and stride >= 1");
+        int rc = harvest_free();
+        if (rc) return rc;
+        ICEMPM_CUDA(cudaMalloc(&harvest_rec_, 2 * (size_t)capacity * sizeof(float4)));
+        ICEMPM_CUDA(cudaMalloc(&harvest_, sizeof(HarvestBuf)));
+        HarvestBuf h{0u, capacity, harvest_rec_};
+        ICEMPM_CUDA(cudaMemcpyAsync(harvest_, &h, sizeof(h), cudaMemcpyHostToDevice, stream_));
+        ICEMPM_CUDA(cudaStreamSynchronize(stream_));
+        harvest_stride_ = stride;
+        kp_.harvest = harvest_;
+        kp_.harvest_stride = stride;
+        invalidate_graphs();
+        return 0;
+    }
+
+    // Copies the records (8 floats each) out, reports how many were offered
+    // (*count may exceed the capacity), and stops recording.
+    int harvest_end(float *records, uint32_t host_cap, uint32_t *count) override
+    {
+        if (!harvest_) return fail(ICEMPM_E_STATE, "no harvest in progress");
+        HarvestBuf h{};
+        ICEMPM_CUDA(cudaMemcpyAsync(&h, harvest_, sizeof(h), cudaMemcpyDeviceToHost, stream_));
+        ICEMPM_CUDA(cudaStreamSynchronize(stream_));
+        const uint32_t m = std::min(std::min(h.count, h.cap), host_cap);
+        if (records && m)
+            ICEMPM_CUDA(cudaMemcpy(records, harvest_rec_, 2 * (size_t)m * sizeof(float4), cudaMemcpyDeviceToHost));
+        if (count) *count = h.count;
+        return harvest_free();
+    }
+
     uint32_t count() const override { return n_real_; }
     int device() const { return opts_.device; }
     cudaStream_t stream() const override { return stream_; }
@@ -561,6 +590,17 @@ public:
     double fixed_scale_p() const override { return kp_.scale_p; }
 
 private:
+    int harvest_free()
+    {
+        if (stream_) ICEMPM_CUDA(cudaStreamSynchronize(stream_));
+        cudaFree(harvest_);
+        cudaFree(harvest_rec_);
+        harvest_ = nullptr;
+        harvest_rec_ = nullptr;
+        kp_.harvest = nullptr;
+        invalidate_graphs();
+        return 0;
+    }
     Grid<Real, Acc> grid() const
     {
         Grid<Real, Acc> g;
@@ -577,7 +617,7 @@ private:
         invalidate_graphs();
         cudaFree(pts_mem_); cudaFree(acc_); cudaFree(vel_); cudaFree(cur_); cudaFree(frc_); cudaFree(status_);
         cudaFree(force_); cudaFree(st_); cudaFree(stage_); cudaFree(keys_[0]); cudaFree(keys_[1]);
-        cudaFree(vals_[0]); cudaFree(vals_[1]); cudaFree(sort_tmp_); cudaFree(runs_); cudaFree(aux_);
+        cudaFree(vals_[0]); cudaFree(vals_[1]); cudaFree(sort_tmp_); cudaFree(harvest_); cudaFree(harvest_rec_); cudaFree(runs_); cudaFree(aux_);
         if (ev0_) cudaEventDestroy(ev0_);
         if (ev1_) cudaEventDestroy(ev1_);
         for (auto &e : evs_) if (e) cudaEventDestroy(e);
@@ -594,6 +634,9 @@ private:
     uint32_t n_real_ = 0;   // points (host slots)
     size_t nc_ = 0;         // allocated entries per point array
     double max_thick_ = 1.0;
+    HarvestBuf *harvest_ = nullptr;   // device record of return-map pairs (null: off)
+    float4 *harvest_rec_ = nullptr;
+    int harvest_stride_ = 1;
     cudaStream_t stream_ = nullptr;
     cudaEvent_t ev0_ = nullptr, ev1_ = nullptr, evs_[3] = {nullptr, nullptr, nullptr};
     void *pts_mem_ = nullptr;

@@ -33,6 +33,8 @@ public:
     virtual uint64_t launches() const = 0;
     virtual double fixed_scale_m() const = 0;
     virtual double fixed_scale_p() const = 0;
+    virtual int harvest_begin(uint32_t capacity, int stride) = 0;
+    virtual int harvest_end(float *records, uint32_t host_cap, uint32_t *count) = 0;
 };
 
 // Ensemble of contexts of one variant stepped together (batch.cuh).

@@ -317,6 +317,49 @@ ICEMPM_API int icempm_batch_get_tuning(icempm_batch_t *batch, icempm_batch_tunin
 ICEMPM_API int icempm_batch_timings(icempm_batch_t *batch, float ms[4]);
 ICEMPM_API int icempm_batch_launch_count(icempm_batch_t *batch, uint64_t *count);
 
+/* ---- Learned return map (no counterpart in the reference)
+ * An MLP 4 -> 64 -> 64 -> 3 (SiLU) that stands in for the projection of a
+ * trial state onto the Drucker-Prager yield surface (wolper_dp's case 3,
+ * kernels.cuh:411-467).  A trial state is 4 floats (sigma1 >= sigma2 of Fe,
+ * Jp_inv, thickness); inputs x = (log sigma1, log sigma2, log Jp_inv,
+ * log thickness), outputs y = (log sigma1'/sigma1, log sigma2'/sigma2,
+ * log Jp_inv'/Jp_inv), both standardised: norm[14] = x mean[4], x std[4],
+ * y mean[3], y std[3].  Parameters: 4675 floats, row-major W1[64][4] b1[64]
+ * W2[64][64] b2[64] W3[3][64] b3[3].  All pointers d_* are device memory of
+ * the caller; calls are asynchronous on `stream` (cudaStream_t, NULL =
+ * default). */
+ICEMPM_API int icempm_mlp_param_count(void);
+/* d_grad += gradient of mean_s sum_o (y_o - y_ref_o)^2 over n standardised
+ * samples d_x[n][4], d_y[n][3]; *d_loss += that loss. */
+ICEMPM_API int icempm_mlp_grad(const float *d_params, const float *d_x, const float *d_y, uint32_t n,
+                               float *d_grad, float *d_loss, void *stream);
+/* One Adam step (beta 0.9 / 0.999, eps 1e-8; t counts from 1). */
+ICEMPM_API int icempm_mlp_adam(float *d_params, const float *d_grad, float *d_m, float *d_v, int32_t t, float lr,
+                               void *stream);
+/* FP32 forward of the standardised outputs d_y[n][3]. */
+ICEMPM_API int icempm_mlp_forward(const float *d_params, const float *d_x, uint32_t n, float *d_y, void *stream);
+/* The exact map on trial states d_trial[n][4] -> d_out[n][4] (sigma1',
+ * sigma2', Jp_inv', 0), in FP32 or (fp64 != 0) FP64 arithmetic. */
+ICEMPM_API int icempm_return_map_exact(const icempm_simparams_t *prms, const float *d_trial, uint32_t n,
+                                       float *d_out, int32_t fp64, void *stream);
+/* The learned map: BF16 tensor-core inference with FP32 accumulation for the
+ * trial states that project onto the yield surface; the others take the exact
+ * closed forms.  A network answer whose yield residual |q' - q_yield(p')| /
+ * q_yield(p') exceeds tol is replaced by the exact map (counted in
+ * *d_fallbacks, which the call adds to).  d_out[n][4] = (sigma1', sigma2',
+ * Jp_inv', 0 exact / 1 network / 2 fallback). */
+ICEMPM_API int icempm_return_map_learned(const icempm_simparams_t *prms, const float *d_params, const float *d_norm,
+                                         const float *d_trial, uint32_t n, float tol, float *d_out,
+                                         uint32_t *d_fallbacks, void *stream);
+/* Training data from a run: from now on the fused kernel records up to
+ * `capacity` projections (trial, projected) of crushed points with
+ * (index + sub-step) % stride == 0.  icempm_harvest_end copies the records
+ * (8 floats each: sigma1, sigma2, Jp_inv, thickness, sigma1', sigma2',
+ * Jp_inv', 3) to `records`, sets *count to the number offered (may exceed
+ * capacity) and stops recording. */
+ICEMPM_API int icempm_harvest_begin(icempm_t *ctx, uint32_t capacity, int32_t stride);
+ICEMPM_API int icempm_harvest_end(icempm_t *ctx, float *records, uint32_t capacity, uint32_t *count);
+
 /* Message of the last failing call on this thread ("" if none). */
 ICEMPM_API const char *icempm_last_error(void);
 

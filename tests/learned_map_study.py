@@ -1,0 +1,115 @@
+"""Learned return map study.
+
+1. Training pairs: projections recorded by the fused kernel from plain-method
+   runs -- the 1M-point ridging scene (1024x512 grid, 2 m/s against the wall)
+   and the config-1 scene on a 2048x1024 grid -- up to --pairs records.
+2. Training: the library's GPU kernels (icempm_mlp_grad + icempm_mlp_adam),
+   minibatch Adam on standardised features.
+3. Evaluation: trial states recorded from a 16M-point compressive ridging
+   scene (8192x2048 grid, h = 1 m, 2 m/s against the wall, --eval-steps
+   sub-steps), mapped by the learned map (BF16 tensor cores, exact fallback
+   above the yield residual) and by the exact map (FP32 and FP64): fallback
+   rate, error of the answers against FP64, device time per trial state.
+
+    python tests/learned_map_study.py [--pairs 20000000] [--eval-steps 500] [--json out.json]
+
+A checker and measurement script (it is not on the product path).
+"""
+import argparse
+import json
+import os
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(HERE))
+
+from icempm_2d_sp_b200 import capi, scenes, surrogate  # noqa: E402
+from icempm_2d_sp_b200.params import Options  # noqa: E402
+
+
+def harvest(sc, steps, capacity, stride, forcing_opts=True):
+    o = Options.default(forcing=sc.options.forcing)
+    if forcing_opts:
+        for f in ("wind_kind", "wind_u", "wind_v", "wind_cx", "wind_cy", "wind_vmax", "wind_radius"):
+            setattr(o, f, getattr(sc.options, f))
+    with capi.Context(sc.prms, sc.status, sc.current, capacity=sc.n, options=o) as ctx:
+        ctx.upload(sc.soa, sc.n)
+        ctx.harvest_begin(capacity, stride)
+        ctx.step(steps, 0)
+        rec, offered = ctx.harvest_end()
+    return rec, offered
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--pairs", type=int, default=20_000_000)
+    ap.add_argument("--eval-steps", type=int, default=500)
+    ap.add_argument("--eval-states", type=int, default=16_000_000)
+    ap.add_argument("--epochs", type=int, default=4)
+    ap.add_argument("--json", default=None)
+    a = ap.parse_args()
+    out = {}
+    t0 = time.time()
+    # 1. training pairs
+    r1, o1 = harvest(scenes.ridging(), 1000, a.pairs, 2)
+    parts = [r1]
+    if len(r1) < a.pairs:
+        sc1 = scenes.config1(gx=2048, gy=1024, n_seeds=500)
+        r2, o2 = harvest(sc1, 200, a.pairs - len(r1), 1)
+        parts.append(r2)
+        out["pairs_config1"] = int(len(r2))
+    rec = np.concatenate(parts)
+    out["pairs"] = int(len(rec))
+    out["pairs_ridging"] = int(len(r1))
+    print(f"# {len(rec)} pairs ({time.time() - t0:.1f} s)", file=sys.stderr)
+    # 2. training
+    x = surrogate.feats(rec[:, :4])
+    y = surrogate.targets(rec[:, :4], rec[:, 4:7])
+    norm = surrogate.Norm.fit(x, y)
+    xs = ((x - norm.x_mean) / norm.x_std).astype(np.float32)
+    ys = ((y - norm.y_mean) / norm.y_std).astype(np.float32)
+    tr = surrogate.Trainer(lr=2e-3)
+    t1 = time.time()
+    hist = tr.fit(xs, ys, epochs=a.epochs, batch=8192)
+    out["train_seconds"] = time.time() - t1
+    out["loss_per_epoch"] = hist
+    params = tr.params()
+    print(f"# trained: loss {hist} ({out['train_seconds']:.1f} s)", file=sys.stderr)
+    # 3. evaluation on the 16M-point ridging scene
+    ev = scenes.ridging(gx=8192, gy=2048, cells_x=4000, cells_y=1000, h=1.0, dt=1e-4, speed=2.0,
+                        steps=a.eval_steps)
+    stride = 1
+    trial, offered = harvest(ev, a.eval_steps, a.eval_states, stride)
+    out["eval_points"] = int(ev.n)
+    out["eval_states"] = int(len(trial))
+    exact64, _ = surrogate.exact_map(ev.prms, trial[:, :4], fp64=True)
+    exact32, ms_exact = surrogate.exact_map(ev.prms, trial[:, :4], fp64=False, repeat=5)
+    out["exact_fp32_ms"] = ms_exact
+    rel = lambda a_, b_: np.abs(a_[:, :3] - b_[:, :3]) / np.abs(b_[:, :3])
+    out["exact_fp32_err_max"] = float(rel(exact32, exact64).max())
+    rows = []
+    for tol in (1e-4, 1e-3, 1e-2):
+        got, nfb, ms = surrogate.learned_map(ev.prms, params, norm, trial[:, :4], tol=tol, repeat=5)
+        how = got[:, 3]
+        net = how == 1.0
+        e = rel(got, exact64)
+        rows.append({"tol": tol, "fallback_rate": float((how == 2.0).mean()), "exact_form_rate": float((how == 0).mean()),
+                     "network_rate": float(net.mean()), "ms": ms,
+                     "err_max_all": float(e.max()), "err_rms_all": float(np.sqrt((e ** 2).mean())),
+                     "err_max_network": float(e[net].max()) if net.any() else 0.0,
+                     "err_rms_network": float(np.sqrt((e[net] ** 2).mean())) if net.any() else 0.0})
+    out["learned"] = rows
+    raw, _, ms_raw = surrogate.learned_map(ev.prms, params, norm, trial[:, :4], tol=1e30, repeat=5)
+    er = rel(raw, exact64)
+    out["network_only"] = {"ms": ms_raw, "err_max": float(er.max()), "err_rms": float(np.sqrt((er ** 2).mean()))}
+    print(json.dumps(out, indent=1))
+    if a.json:
+        with open(a.json, "w") as f:
+            json.dump(out, f, indent=1)
+
+
+if __name__ == "__main__":
+    main()

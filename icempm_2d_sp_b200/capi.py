@@ -23,8 +23,17 @@ EXPORTS = [
     "icempm_batch_create", "icempm_batch_destroy", "icempm_batch_step", "icempm_batch_autotune",
     "icempm_batch_set_tuning", "icempm_batch_get_tuning", "icempm_batch_timings", "icempm_batch_launch_count",
     "icempm_mlp_param_count", "icempm_mlp_grad", "icempm_mlp_adam", "icempm_mlp_forward", "icempm_return_map_exact",
-    "icempm_return_map_learned", "icempm_harvest_begin", "icempm_harvest_end",
+    "icempm_return_map_learned", "icempm_harvest_begin", "icempm_harvest_end", "icempm_prepare_frame",
 ]
+
+FRAME_CHANNELS = ("point_density", "mass", "vx", "vy", "Jpinv", "P", "Q", "r", "g", "b")
+
+
+class FrameBuffers(C.Structure):
+    """icempm_frame_t"""
+    _fields_ = [(k, C.POINTER(C.c_float)) for k in FRAME_CHANNELS] + [
+        ("rgb", C.POINTER(C.c_uint8)), ("mass_mask", C.POINTER(C.c_uint8)), ("count", C.POINTER(C.c_uint8)),
+        ("forces_per_region", C.POINTER(C.c_float))]
 
 
 class BatchTuning(C.Structure):
@@ -101,6 +110,8 @@ def load(path: str = LIB_PATH):
                                                 C.c_void_p, C.c_void_p, C.c_void_p]),
         "icempm_harvest_begin": (C.c_int, [h, C.c_uint32, C.c_int32]),
         "icempm_harvest_end": (C.c_int, [h, C.POINTER(C.c_float), C.c_uint32, C.POINTER(C.c_uint32)]),
+        "icempm_prepare_frame": (C.c_int, [h, C.POINTER(C.c_uint32), C.c_uint32, C.c_int32,
+                                           C.POINTER(FrameBuffers)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -145,6 +156,25 @@ class Context:
         """Record return-map projections of the following steps (icempm_harvest_begin)."""
         check(self._L.icempm_harvest_begin(self.h, int(capacity), int(stride)))
         self._harvest_cap = int(capacity)
+
+    def prepare_frame(self, elapsed_steps, colors=None):
+        """Saved-frame grid arrays (icempm_prepare_frame) as numpy arrays."""
+        out = {k: np.zeros(self.G, np.float32) for k in FRAME_CHANNELS}
+        out["rgb"] = np.zeros(3 * self.G, np.uint8)
+        out["mass_mask"] = np.zeros(self.G, np.uint8)
+        out["count"] = np.zeros(self.G, np.uint8)
+        out["forces_per_region"] = np.zeros(2 * 100, np.float32)
+        fb = FrameBuffers()
+        for k in FRAME_CHANNELS + ("forces_per_region",):
+            setattr(fb, k, out[k].ctypes.data_as(C.POINTER(C.c_float)))
+        for k in ("rgb", "mass_mask", "count"):
+            setattr(fb, k, out[k].ctypes.data_as(C.POINTER(C.c_uint8)))
+        cp, nc = None, 0
+        if colors is not None:
+            colors = np.ascontiguousarray(colors, np.uint32)
+            cp, nc = colors.ctypes.data_as(C.POINTER(C.c_uint32)), len(colors)
+        check(self._L.icempm_prepare_frame(self.h, cp, nc, int(elapsed_steps), C.byref(fb)))
+        return out
 
     def harvest_end(self):
         """The recorded (trial, projected) pairs as float32 [count, 8], and how many were offered."""

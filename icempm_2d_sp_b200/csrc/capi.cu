@@ -242,6 +242,14 @@ int icempm_device_count(int *count)
     return ICEMPM_OK;
 }
 
+int icempm_prepare_frame(icempm_t *ctx, const uint32_t *point_colors_rgb, uint32_t ncolors, int32_t elapsed_steps,
+                         icempm_frame_t *out)
+{
+    ICEMPM_GUARD_CTX(ctx);
+    if (!out) return fail(ICEMPM_E_ARG, "out is null");
+    ICEMPM_TRY(ctx->eng->prepare_frame(point_colors_rgb, ncolors, elapsed_steps, out));
+}
+
 int icempm_harvest_begin(icempm_t *ctx, uint32_t capacity, int32_t stride)
 {
     ICEMPM_GUARD_CTX(ctx);

@@ -10,6 +10,7 @@
 #include <algorithm>
 
 #include "transfer.cuh"
+#include "frame.cuh"
 #include "engine_iface.h"
 
 namespace icempm {
@@ -582,6 +583,59 @@ public:
         return harvest_free();
     }
 
+    // Saved-frame grid arrays (frame.cuh) into the caller's host buffers.
+    int prepare_frame(const uint32_t *colors, uint32_t ncolors, int elapsed, icempm_frame_t *out) override
+    {
+        if (elapsed <= 0) return fail(ICEMPM_E_ARG, "elapsed_steps must be > 0");
+        if (!frame_mem_) {
+            const size_t bytes = G_ * (kFrameChannels * sizeof(float) + sizeof(uint32_t) + 5) +
+                                 2 * ICEMPM_MAX_REGIONS * sizeof(float) + 256;
+            ICEMPM_CUDA(cudaMalloc(&frame_mem_, bytes));
+            char *b = (char *)frame_mem_;
+            for (int c = 0; c < kFrameChannels; c++) { frame_.ch[c] = (float *)b; b += G_ * sizeof(float); }
+            frame_.count = (uint32_t *)b; b += G_ * sizeof(uint32_t);
+            frame_.region_force = (float *)b; b += 2 * ICEMPM_MAX_REGIONS * sizeof(float);
+            frame_.rgb = (uint8_t *)b; b += 3 * G_;
+            frame_.mask = (uint8_t *)b; b += G_;
+            frame_.count8 = (uint8_t *)b;
+        }
+        if (colors && ncolors) {
+            if (ncolors > colors_cap_) {
+                cudaFree(colors_);
+                colors_ = nullptr;
+                ICEMPM_CUDA(cudaMalloc(&colors_, (size_t)ncolors * sizeof(uint32_t)));
+                colors_cap_ = ncolors;
+            }
+            ICEMPM_CUDA(cudaMemcpyAsync(colors_, colors, (size_t)ncolors * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                                        stream_));
+        }
+        const size_t zero_bytes = G_ * (kFrameChannels * sizeof(float) + sizeof(uint32_t)) +
+                                  2 * ICEMPM_MAX_REGIONS * sizeof(float);
+        ICEMPM_CUDA(cudaMemsetAsync(frame_mem_, 0, zero_bytes, stream_));
+        if (n_ > 0) {
+            k_frame_scatter<Real><<<(n_ + 255) / 256, 256, 0, stream_>>>(
+                pts_[par_], (int)n_, gx_, gy_, Real(prms_.ParticleMass), (colors && ncolors) ? colors_ : nullptr,
+                (colors && ncolors) ? ncolors : 0u, frame_);
+            launches_++;
+        }
+        k_frame_finish<<<(unsigned)((G_ + 255) / 256), 256, 0, stream_>>>(
+            frame_, status_, force_, (double)elapsed * prms_.InitialTimeStep, (long long)G_);
+        launches_++;
+        ICEMPM_CUDA(cudaGetLastError());
+        float *const dst[kFrameChannels] = {out->point_density, out->mass, out->vx, out->vy, out->Jpinv,
+                                            out->P, out->Q, out->r, out->g, out->b};
+        for (int c = 0; c < kFrameChannels; c++)
+            if (dst[c]) ICEMPM_CUDA(cudaMemcpyAsync(dst[c], frame_.ch[c], G_ * sizeof(float), cudaMemcpyDeviceToHost, stream_));
+        if (out->rgb) ICEMPM_CUDA(cudaMemcpyAsync(out->rgb, frame_.rgb, 3 * G_, cudaMemcpyDeviceToHost, stream_));
+        if (out->mass_mask) ICEMPM_CUDA(cudaMemcpyAsync(out->mass_mask, frame_.mask, G_, cudaMemcpyDeviceToHost, stream_));
+        if (out->count) ICEMPM_CUDA(cudaMemcpyAsync(out->count, frame_.count8, G_, cudaMemcpyDeviceToHost, stream_));
+        if (out->forces_per_region)
+            ICEMPM_CUDA(cudaMemcpyAsync(out->forces_per_region, frame_.region_force,
+                                        2 * ICEMPM_MAX_REGIONS * sizeof(float), cudaMemcpyDeviceToHost, stream_));
+        ICEMPM_CUDA(cudaStreamSynchronize(stream_));
+        return 0;
+    }
+
     uint32_t count() const override { return n_real_; }
     int device() const { return opts_.device; }
     cudaStream_t stream() const override { return stream_; }
@@ -617,7 +671,7 @@ private:
         invalidate_graphs();
         cudaFree(pts_mem_); cudaFree(acc_); cudaFree(vel_); cudaFree(cur_); cudaFree(frc_); cudaFree(status_);
         cudaFree(force_); cudaFree(st_); cudaFree(stage_); cudaFree(keys_[0]); cudaFree(keys_[1]);
-        cudaFree(vals_[0]); cudaFree(vals_[1]); cudaFree(sort_tmp_); cudaFree(harvest_); cudaFree(harvest_rec_); cudaFree(runs_); cudaFree(aux_);
+        cudaFree(vals_[0]); cudaFree(vals_[1]); cudaFree(sort_tmp_); cudaFree(harvest_); cudaFree(harvest_rec_); cudaFree(frame_mem_); cudaFree(colors_); cudaFree(runs_); cudaFree(aux_);
         if (ev0_) cudaEventDestroy(ev0_);
         if (ev1_) cudaEventDestroy(ev1_);
         for (auto &e : evs_) if (e) cudaEventDestroy(e);
@@ -634,6 +688,10 @@ private:
     uint32_t n_real_ = 0;   // points (host slots)
     size_t nc_ = 0;         // allocated entries per point array
     double max_thick_ = 1.0;
+    void *frame_mem_ = nullptr;       // saved-frame grid arrays (allocated on first use)
+    FrameOut frame_{};
+    uint32_t *colors_ = nullptr;
+    uint32_t colors_cap_ = 0;
     HarvestBuf *harvest_ = nullptr;   // device record of return-map pairs (null: off)
     float4 *harvest_rec_ = nullptr;
     int harvest_stride_ = 1;

@@ -35,6 +35,7 @@ public:
     virtual double fixed_scale_p() const = 0;
     virtual int harvest_begin(uint32_t capacity, int stride) = 0;
     virtual int harvest_end(float *records, uint32_t host_cap, uint32_t *count) = 0;
+    virtual int prepare_frame(const uint32_t *colors, uint32_t ncolors, int elapsed, icempm_frame_t *out) = 0;
 };
 
 // Ensemble of contexts of one variant stepped together (batch.cuh).

@@ -283,6 +283,26 @@ ICEMPM_API int icempm_launch_count(icempm_t *ctx, uint64_t *count);
 ICEMPM_API int icempm_cell_order_noalloc(const uint32_t *d_cell, const uint32_t *d_utility, uint32_t n,
                                          int32_t grid_y, uint32_t *d_order, uint32_t *d_count, void *stream);
 
+/* Grid arrays of a saved frame (SnapshotManager::PrepareFrameArrays,
+ * snapshotmanager.cpp:623-765), computed on the GPU from the points on the
+ * device.  Each pointer is a host buffer of the caller (NULL skips that
+ * array): G = GridXTotal * GridYTotal floats for the ten channels, 3G bytes
+ * of interleaved colour, G bytes of mass mask and of points per cell, and
+ * 2 * ICEMPM_MAX_REGIONS floats of (fx, fy) boundary force per region. */
+typedef struct icempm_frame_t {
+    float *point_density, *mass, *vx, *vy, *Jpinv, *P, *Q, *r, *g, *b;
+    uint8_t *rgb;
+    uint8_t *mass_mask;
+    uint8_t *count;
+    float *forces_per_region;
+} icempm_frame_t;
+
+/* point_colors_rgb[pid] = 0xRRGGBB by point id (GPU_Implementation5::
+ * point_colors_rgb); NULL or ids >= ncolors colour points white.  The boundary
+ * forces are divided by elapsed_steps * dt as icempm_get_boundary_forces does. */
+ICEMPM_API int icempm_prepare_frame(icempm_t *ctx, const uint32_t *point_colors_rgb, uint32_t ncolors,
+                                    int32_t elapsed_steps, icempm_frame_t *out);
+
 /* ---- Ensembles (no counterpart in the reference) --------
  * Many independent scenes advanced together: one launch of the grid update
  * and one of the fused kernel per sub-step cover every scene of the batch,

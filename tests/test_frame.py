@@ -1,0 +1,77 @@
+"""Saved-frame grid arrays (icempm_prepare_frame) against the CPU restatement
+of SnapshotManager::PrepareFrameArrays (oracle/frame_reference.py).
+
+Tolerances: the ten channels within 1e-4 of each channel's largest magnitude
+(FP32 sums in another order), Jpinv (an average of values near 1, minus 1)
+within 2e-6 absolute; mass mask and points per cell identical except
+nodes whose density sits within 1e-5 of the 0.1 threshold; colour within one
+unit (truncation after FP32 blending); region forces within 1e-4 relative.
+"""
+import numpy as np
+import pytest
+
+from icempm_2d_sp_b200 import scenes, hssoa as H
+from icempm_2d_sp_b200.params import Options, SimParams, IDX_UTILITY, STATUS_DISABLED
+from oracle import frame_reference as fr
+
+
+def test_reference_restatement_single_point():
+    """KAT of the restatement: one point at a cell centre spreads the B-spline
+    weights 1/8, 3/4, 1/8 per axis: density 9/16 at the centre node."""
+    sc = scenes.random_state(seed=1, gx=16, gy=16)
+    soa = sc.soa[:, :1].copy()
+    cell = (8 << 16) | 8
+    soa[1, 0] = np.frombuffer(np.uint64(cell).tobytes(), np.float64)[0]
+    soa[0, 0] = 0.0
+    soa[2, 0] = 0.0
+    soa[6, 0] = soa[7, 0] = 0.0
+    soa[8, 0], soa[9, 0] = 2.0, -1.0
+    status = np.full(256, 100, np.uint8)
+    out = fr.prepare_frame(sc.prms, soa, 1, status, np.zeros(512), colors=np.array([0x102030], np.uint32))
+    c = 8 * 16 + 8
+    assert abs(out["density"][c] - 0.5625) < 1e-12
+    assert abs(out["vx"][c] - 2.0) < 1e-12 and abs(out["vy"][c] + 1.0) < 1e-12
+    assert out["count"][c] == 1 and out["mass_mask"][c] == 1
+    # a side node holds 3/4 * 1/8 = 0.09375 < 0.1: masked and zeroed, colour blended with water
+    assert out["mass_mask"][c + 1] == 0 and out["density"][c + 1] == 0.0
+    a = 0.09375
+    assert out["rgb"][3 * (c + 1)] == int(a * 0x10 + (1 - a) * 0x15)
+    assert abs(out["r"][c] - 0x10) < 1e-9 and abs(out["b"][c] - 0x30) < 1e-9
+
+
+@pytest.mark.gpu
+def test_frame_arrays_match_restatement():
+    from icempm_2d_sp_b200 import capi
+    capi.load()
+    if capi.device_count() < 1:
+        pytest.fail("no CUDA device visible to the library")
+    sc = scenes.ridging(gx=256, gy=128, cells_x=120, cells_y=100, speed=2.0)
+    rng = np.random.default_rng(5)
+    soa = sc.soa.copy()
+    util = H.get_u32(soa, IDX_UTILITY, sc.n).copy()
+    util[rng.random(sc.n) < 0.05] |= STATUS_DISABLED            # some disabled points
+    H.set_u32(soa, IDX_UTILITY, util, sc.n)
+    colors = rng.integers(0, 1 << 24, sc.n).astype(np.uint32)
+    steps = 30
+    with capi.Context(sc.prms, sc.status, sc.current, capacity=sc.n, options=Options.default()) as ctx:
+        ctx.upload(soa, sc.n)
+        ctx.step(steps, 0)
+        got = ctx.prepare_frame(steps, colors)
+        got2 = ctx.prepare_frame(steps, colors)                 # repeatable
+        out, m = ctx.download(np.zeros_like(soa))
+        forces = ctx.boundary_forces(steps)
+    ref = fr.prepare_frame(sc.prms, out, m, sc.status, forces, colors)
+    for k in capi.FRAME_CHANNELS:
+        rk = "density" if k == "point_density" else k
+        scale = max(np.abs(ref[rk]).max(), 1e-30)
+        # Jpinv is sum(w Jp) / sum(w) - 1 with Jp ~ 1: FP32 sums leave ~1e-7 absolute
+        tol = 2e-6 if k == "Jpinv" else 1e-4 * scale
+        assert np.abs(got[k] - ref[rk]).max() <= tol, k
+        assert np.abs(got2[k] - got[k]).max() <= tol, k
+    border = np.abs(ref["density"] - 0.1) < 1e-5
+    assert np.array_equal(got["mass_mask"][~border], ref["mass_mask"][~border])
+    assert np.array_equal(got["count"], ref["count"])
+    assert np.abs(got["rgb"].astype(int) - ref["rgb"].astype(int)).max() <= 1
+    rf = ref["forces_per_region"]
+    assert np.abs(got["forces_per_region"] - rf).max() <= 1e-4 * max(np.abs(rf).max(), 1e-30)
+    assert np.abs(rf).max() > 0                                 # the wall took load

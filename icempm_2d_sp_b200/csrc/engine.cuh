@@ -812,8 +812,9 @@ __device__ __noinline__ void harvest_record(HarvestBuf *hb, const MatT<Real> &m,
 // scene's arrays, whose A, H, K are in stage `s`.  With one stage, the next
 // chunk (`next`, arrays Pn from base_n) is fetched into it once its points
 // are read.  Error bits and the count of newly disabled points accumulate
-// into err, perr, ndis.
-template <class Real, class Acc, int BT, int PPT, int CAP, int STAGES>
+// into err, perr, ndis.  HARVEST: the instance that records return-map pairs
+// (kept out of the ordinary instance, whose registers it would crowd).
+template <class Real, class Acc, int BT, int PPT, int CAP, int STAGES, bool HARVEST>
 __device__ __forceinline__ void fused_chunk(ChunkSmem<Real, Acc, BT, PPT, CAP, STAGES> &sm, int s,
                                             const KParams<Real> &kp, const Pts<Real> &P, const Grid<Real, Acc> &G,
                                             uint32_t base, int n, int step, bool recordPQ, bool store_vc, bool next,
@@ -958,7 +959,7 @@ __device__ __forceinline__ void fused_chunk(ChunkSmem<Real, Acc, BT, PPT, CAP, S
             const SvdH<Real> sv = svd_h(H);
             const Real jp0 = Jp;
             wolper_dp(kp.mat, thick, p_tr, q_tr, k, sv, H, Jp);
-            if (kp.harvest && (i + (uint32_t)step) % (uint32_t)kp.harvest_stride == 0u)
+            if (HARVEST && kp.harvest && (i + (uint32_t)step) % (uint32_t)kp.harvest_stride == 0u)
                 harvest_record(kp.harvest, kp.mat, sv, p_tr, q_tr, jp0, thick, H, Jp);
             if (isnan((H.a00 + H.a10) + (H.a01 + H.a11))) err |= kErrFeNan;
             k = kinematics(H);
@@ -1053,7 +1054,7 @@ __device__ __forceinline__ void fused_chunk(ChunkSmem<Real, Acc, BT, PPT, CAP, S
     tile_flush<Acc, CAP, BT>(T, G.acc, kp.gx, kp.gy);
 }
 
-template <class Real, class Acc, int BT, int PPT, int CAP, int STAGES>
+template <class Real, class Acc, int BT, int PPT, int CAP, int STAGES, bool HARVEST>
 __global__ void __launch_bounds__(BT, (sizeof(Real) == 8 ? 1 : ICEMPM_FUSED_MINB))
 k_g2p_p2g(KParams<Real> kp, Pts<Real> P, Grid<Real, Acc> G, DevStatus *st, int n, int nchunks)
 {
@@ -1087,7 +1088,7 @@ k_g2p_p2g(KParams<Real> kp, Pts<Real> P, Grid<Real, Acc> G, DevStatus *st, int n
         const bool next = c + (int)gridDim.x < nchunks;
         const uint32_t base_n = (uint32_t)(c + (int)gridDim.x) * CH;
         if (STAGES == 2 && tid == 0 && next) fetch_chunk(sm.stage[s ^ 1], P, base_n, CH, &sm.mbar[s ^ 1]);
-        fused_chunk<Real, Acc, BT, PPT, CAP, STAGES>(sm, s, kp, P, G, (uint32_t)c * CH, n, step, recordPQ, store_vc,
+        fused_chunk<Real, Acc, BT, PPT, CAP, STAGES, HARVEST>(sm, s, kp, P, G, (uint32_t)c * CH, n, step, recordPQ, store_vc,
                                                      next, P, base_n, err, perr, ndis);
     }
     warp_flush_status(st, err, perr, ndis);
@@ -1178,7 +1179,7 @@ k_g2p_p2g_batch(const SceneDesc<Real, Acc> *__restrict__ scenes, const int *__re
         const uint32_t base_n = (uint32_t)(cn - Sn.chunk0) * CH;
         if (STAGES == 2 && tid == 0 && next) fetch_chunk(sm.stage[s ^ 1], Sn.P, base_n, CH, &sm.mbar[s ^ 1]);
         const bool recordPQ = S.kp.update_every > 0 && (step % S.kp.update_every) == 0;
-        fused_chunk<Real, Acc, BT, PPT, CAP, STAGES>(sm, s, S.kp, S.P, S.G, (uint32_t)(c - S.chunk0) * CH, S.n, step,
+        fused_chunk<Real, Acc, BT, PPT, CAP, STAGES, false>(sm, s, S.kp, S.P, S.G, (uint32_t)(c - S.chunk0) * CH, S.n, step,
                                                      recordPQ, store_vc, next, Sn.P, base_n, err, perr, ndis);
         warp_flush_status(S.st, err, perr, ndis);
     }

@@ -120,8 +120,10 @@ public:
         tile_.tx = 8; tile_.ty = BT * PPT / 32;
         tile_.ntiles_y = (gy_ + tile_.ty - 1) / tile_.ty;
         // persistent grid of the fused kernel: as many CTAs as fit on the device
-        auto kern = k_g2p_p2g<Real, Acc, BT, PPT, CAP, STAGES>;
+        auto kern = k_g2p_p2g<Real, Acc, BT, PPT, CAP, STAGES, false>;
         ICEMPM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(FusedSmem)));
+        ICEMPM_CUDA(cudaFuncSetAttribute(k_g2p_p2g<Real, Acc, BT, PPT, CAP, STAGES, true>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(FusedSmem)));
         int per_sm = 0, sms = 0;
         ICEMPM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, BT, sizeof(FusedSmem)));
         ICEMPM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, o.device));
@@ -282,8 +284,12 @@ public:
     {
         const int nchunks = (int)(((size_t)n_ + CH - 1) / CH);
         const unsigned nb = (unsigned)(ICEMPM_FUSED_PERSIST ? std::min(nchunks, fused_ctas_) : nchunks);
-        k_g2p_p2g<Real, Acc, BT, PPT, CAP, STAGES>
-            <<<nb, BT, sizeof(FusedSmem), stream_>>>(kp_, pts_[par_], grid(), st_, (int)n_, nchunks);
+        if (kp_.harvest)
+            k_g2p_p2g<Real, Acc, BT, PPT, CAP, STAGES, true>
+                <<<nb, BT, sizeof(FusedSmem), stream_>>>(kp_, pts_[par_], grid(), st_, (int)n_, nchunks);
+        else
+            k_g2p_p2g<Real, Acc, BT, PPT, CAP, STAGES, false>
+                <<<nb, BT, sizeof(FusedSmem), stream_>>>(kp_, pts_[par_], grid(), st_, (int)n_, nchunks);
         launches_++;
     }
     int prime()

@@ -24,6 +24,7 @@ EXPORTS = [
     "icempm_batch_set_tuning", "icempm_batch_get_tuning", "icempm_batch_timings", "icempm_batch_launch_count",
     "icempm_mlp_param_count", "icempm_mlp_grad", "icempm_mlp_adam", "icempm_mlp_forward", "icempm_return_map_exact",
     "icempm_return_map_learned", "icempm_harvest_begin", "icempm_harvest_end", "icempm_prepare_frame",
+    "icempm_set_flow_frames", "icempm_set_wind_frames", "icempm_set_forcing_time", "icempm_get_forcing",
 ]
 
 FRAME_CHANNELS = ("point_density", "mass", "vx", "vy", "Jpinv", "P", "Q", "r", "g", "b")
@@ -73,6 +74,11 @@ def load(path: str = LIB_PATH):
         "icempm_upload_points": (C.c_int, [h, dp, C.c_uint32, C.c_uint32, C.c_int32]),
         "icempm_update_constants": (C.c_int, [h, sp]),
         "icempm_set_current": (C.c_int, [h, dp]),
+        "icempm_set_flow_frames": (C.c_int, [h, dp, dp]),
+        "icempm_set_wind_frames": (C.c_int, [h, C.POINTER(C.c_float), C.c_int32, C.c_int32, C.c_double,
+                                             C.c_double, C.c_double]),
+        "icempm_set_forcing_time": (C.c_int, [h, C.c_double, C.c_double]),
+        "icempm_get_forcing": (C.c_int, [h, dp, dp]),
         "icempm_step": (C.c_int, [h, C.c_int32, C.c_int32]),
         "icempm_download_points": (C.c_int, [h, dp, C.c_uint32, C.POINTER(C.c_uint32)]),
         "icempm_get_status": (C.c_int, [h, C.POINTER(C.c_uint32), C.POINTER(C.c_int32)]),
@@ -228,6 +234,36 @@ class Context:
     def set_current(self, current):
         cur = None if current is None else np.ascontiguousarray(current, dtype=np.float64)
         check(self._L.icempm_set_current(self.h, _dp(cur)))
+
+    def set_flow_frames(self, current_a, current_b=None):
+        """Current frames a, b ([2G] doubles each, vx block then vy block)."""
+        a = None if current_a is None else np.ascontiguousarray(current_a, dtype=np.float64)
+        b = None if current_b is None else np.ascontiguousarray(current_b, dtype=np.float64)
+        for x in (a, b):
+            if x is not None and x.size != 2 * self.G:
+                raise ValueError(f"current frame holds {x.size} values, expected {2 * self.G}")
+        check(self._L.icempm_set_flow_frames(self.h, _dp(a), _dp(b)))
+
+    def set_wind_frames(self, wind, cell=1.0, x0=0.0, y0=0.0):
+        """Wind frames float32 [rows, cols, 4] = {u_a, v_a, u_b, v_b}; None drops them."""
+        if wind is None:
+            check(self._L.icempm_set_wind_frames(self.h, None, 0, 0, 1.0, 0.0, 0.0))
+            return
+        w = np.ascontiguousarray(wind, dtype=np.float32)
+        if w.ndim != 3 or w.shape[2] != 4:
+            raise ValueError("wind frames must be [rows, cols, 4]")
+        self._wind = w
+        check(self._L.icempm_set_wind_frames(self.h, w.ctypes.data_as(C.POINTER(C.c_float)), w.shape[0],
+                                             w.shape[1], float(cell), float(x0), float(y0)))
+
+    def set_forcing_time(self, tc, tw=None):
+        check(self._L.icempm_set_forcing_time(self.h, float(tc), float(tc if tw is None else tw)))
+
+    def get_forcing(self):
+        """(current [2G], wind stress [2G]) as the sub-steps read them."""
+        cur, st = np.zeros(2 * self.G), np.zeros(2 * self.G)
+        check(self._L.icempm_get_forcing(self.h, _dp(cur), _dp(st)))
+        return cur, st
 
     def step(self, nsteps: int, first_step: int = 0):
         check(self._L.icempm_step(self.h, int(nsteps), int(first_step)))

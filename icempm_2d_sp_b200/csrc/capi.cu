@@ -134,6 +134,31 @@ int icempm_set_current(icempm_t *ctx, const double *current_vxvy)
     ICEMPM_TRY(ctx->eng->set_current(current_vxvy));
 }
 
+int icempm_set_flow_frames(icempm_t *ctx, const double *current_a, const double *current_b)
+{
+    ICEMPM_GUARD_CTX(ctx);
+    ICEMPM_TRY(ctx->eng->set_flow_frames(current_a, current_b));
+}
+
+int icempm_set_wind_frames(icempm_t *ctx, const float *wind, int32_t rows, int32_t cols, double cell, double x0,
+                           double y0)
+{
+    ICEMPM_GUARD_CTX(ctx);
+    ICEMPM_TRY(ctx->eng->set_wind_frames(wind, rows, cols, cell, x0, y0));
+}
+
+int icempm_set_forcing_time(icempm_t *ctx, double tc, double tw)
+{
+    ICEMPM_GUARD_CTX(ctx);
+    ICEMPM_TRY(ctx->eng->set_forcing_time(tc, tw));
+}
+
+int icempm_get_forcing(icempm_t *ctx, double *current_vxvy, double *wind_stress_xy)
+{
+    ICEMPM_GUARD_CTX(ctx);
+    ICEMPM_TRY(ctx->eng->get_forcing(current_vxvy, wind_stress_xy));
+}
+
 int icempm_step(icempm_t *ctx, int32_t nsteps, int32_t first_step)
 {
     ICEMPM_GUARD_CTX(ctx);

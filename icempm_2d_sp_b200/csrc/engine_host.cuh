@@ -11,6 +11,7 @@
 
 #include "transfer.cuh"
 #include "frame.cuh"
+#include "forcing.cuh"
 #include "engine_iface.h"
 
 namespace icempm {
@@ -204,6 +205,65 @@ public:
         ICEMPM_CUDA(cudaMemcpyAsync(cur_, h.data(), G_ * sizeof(V2<Real>), cudaMemcpyHostToDevice, stream_));
         ICEMPM_CUDA(cudaMemcpyAsync(frc_, f.data(), G_ * sizeof(V4<Real>), cudaMemcpyHostToDevice, stream_));
         ICEMPM_CUDA(cudaStreamSynchronize(stream_));
+        // the extended forcing enters the P2G: a P2G already done for the next step is stale
+        if (opts_.forcing == ICEMPM_FORCING_EXTENDED) primed_ = false;
+        return 0;
+    }
+
+    // ---- time-varying forcing (forcing.cuh) ----
+    int set_flow_frames(const double *a, const double *b) override
+    {
+        if (!a && b) return fail(ICEMPM_E_ARG, "current frame b given without frame a");
+        if (!a) { cudaFree(flow_ab_); flow_ab_ = nullptr; return 0; }
+        if (!b) b = a;
+        if (!flow_ab_) ICEMPM_CUDA(cudaMalloc(&flow_ab_, 4 * G_ * sizeof(double)));
+        ICEMPM_CUDA(cudaMemcpyAsync(flow_ab_, a, 2 * G_ * sizeof(double), cudaMemcpyHostToDevice, stream_));
+        ICEMPM_CUDA(cudaMemcpyAsync(flow_ab_ + 2 * G_, b, 2 * G_ * sizeof(double), cudaMemcpyHostToDevice, stream_));
+        ICEMPM_CUDA(cudaStreamSynchronize(stream_));
+        return 0;
+    }
+    int set_wind_frames(const float *w, int rows, int cols, double cell, double x0, double y0) override
+    {
+        if (!w) { cudaFree((void *)wind_.w); wind_ = WindGrid{}; wind_cap_ = 0; return 0; }
+        if (rows < 1 || cols < 1 || (long long)rows * cols > (1LL << 28))
+            return fail(ICEMPM_E_ARG, "wind grid rows and cols must be in 1..2^28 samples");
+        if (!(cell > 0) || !std::isfinite(cell) || !std::isfinite(x0) || !std::isfinite(y0))
+            return fail(ICEMPM_E_ARG, "wind grid spacing must be finite and > 0, origin finite");
+        const size_t ns = (size_t)rows * cols;
+        if (ns > wind_cap_) {
+            cudaFree((void *)wind_.w);
+            wind_.w = nullptr;
+            ICEMPM_CUDA(cudaMalloc((void **)&wind_.w, ns * sizeof(float4)));
+            wind_cap_ = ns;
+        }
+        ICEMPM_CUDA(cudaMemcpyAsync((void *)wind_.w, w, ns * sizeof(float4), cudaMemcpyHostToDevice, stream_));
+        ICEMPM_CUDA(cudaStreamSynchronize(stream_));
+        wind_.rows = rows; wind_.cols = cols; wind_.cell = cell; wind_.x0 = x0; wind_.y0 = y0;
+        return 0;
+    }
+    int set_forcing_time(double tc, double tw) override
+    {
+        if (!flow_ab_ && !wind_.w) return fail(ICEMPM_E_STATE, "no current or wind frames set");
+        if (!(tc >= 0 && tc <= 1) || !(tw >= 0 && tw <= 1))
+            return fail(ICEMPM_E_ARG, "interpolation weights must be in [0, 1]");
+        const unsigned nb = (unsigned)((G_ + 255) / 256);
+        k_blend_forcing<Real><<<nb, 256, 0, stream_>>>((long long)G_, gy_, prms_.cellsize, flow_ab_,
+                                                      flow_ab_ ? flow_ab_ + 2 * G_ : nullptr, tc, wind_, tw,
+                                                      opts_.air_density * opts_.air_drag_coeff, cur_, frc_);
+        ICEMPM_CUDA(cudaGetLastError());
+        launches_++;
+        if (opts_.forcing == ICEMPM_FORCING_EXTENDED) primed_ = false;
+        return 0;
+    }
+    int get_forcing(double *cur, double *stress) override
+    {
+        std::vector<V4<Real>> f(G_);
+        ICEMPM_CUDA(cudaMemcpyAsync(f.data(), frc_, G_ * sizeof(V4<Real>), cudaMemcpyDeviceToHost, stream_));
+        ICEMPM_CUDA(cudaStreamSynchronize(stream_));
+        for (size_t i = 0; i < G_; i++) {
+            if (cur) { cur[i] = (double)f[i].x; cur[G_ + i] = (double)f[i].y; }
+            if (stress) { stress[i] = (double)f[i].z; stress[G_ + i] = (double)f[i].w; }
+        }
         return 0;
     }
 
@@ -678,6 +738,7 @@ private:
         cudaFree(pts_mem_); cudaFree(acc_); cudaFree(vel_); cudaFree(cur_); cudaFree(frc_); cudaFree(status_);
         cudaFree(force_); cudaFree(st_); cudaFree(stage_); cudaFree(keys_[0]); cudaFree(keys_[1]);
         cudaFree(vals_[0]); cudaFree(vals_[1]); cudaFree(sort_tmp_); cudaFree(harvest_); cudaFree(harvest_rec_); cudaFree(frame_mem_); cudaFree(colors_); cudaFree(runs_); cudaFree(aux_);
+        cudaFree(flow_ab_); cudaFree((void *)wind_.w);
         if (ev0_) cudaEventDestroy(ev0_);
         if (ev1_) cudaEventDestroy(ev1_);
         for (auto &e : evs_) if (e) cudaEventDestroy(e);
@@ -709,6 +770,9 @@ private:
     Acc *acc_ = nullptr;   // mass, x- and y-momentum arrays of G_ each
     V2<Real> *vel_ = nullptr, *cur_ = nullptr;
     V4<Real> *frc_ = nullptr;
+    double *flow_ab_ = nullptr;   // current frames a, b (2 G_ doubles each), null: static current
+    WindGrid wind_{};             // wind frames, null samples: static wind
+    size_t wind_cap_ = 0;
     uint8_t *status_ = nullptr;
     double2 *force_ = nullptr;
     DevStatus *st_ = nullptr;

@@ -36,6 +36,10 @@ public:
     virtual int harvest_begin(uint32_t capacity, int stride) = 0;
     virtual int harvest_end(float *records, uint32_t host_cap, uint32_t *count) = 0;
     virtual int prepare_frame(const uint32_t *colors, uint32_t ncolors, int elapsed, icempm_frame_t *out) = 0;
+    virtual int set_flow_frames(const double *a, const double *b) = 0;
+    virtual int set_wind_frames(const float *w, int rows, int cols, double cell, double x0, double y0) = 0;
+    virtual int set_forcing_time(double tc, double tw) = 0;
+    virtual int get_forcing(double *cur, double *stress) = 0;
 };
 
 // Ensemble of contexts of one variant stepped together (batch.cuh).

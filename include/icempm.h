@@ -198,6 +198,41 @@ ICEMPM_API int icempm_update_constants(icempm_t *ctx, const icempm_simparams_t *
  * gpu_partition.cpp:174-196): 2*GridX*GridY doubles, vx block then vy block. */
 ICEMPM_API int icempm_set_current(icempm_t *ctx, const double *current_vxvy);
 
+/* Time-varying current and wind.  The reference reads one static current
+ * field (WindAndCurrentInterpolator::ReadStaticFlowData,
+ * windandcurrentinterpolator.cpp:20-63), leaves SetTime unfinished (66-70:
+ * "return whether data needs to be copied to GPU") and keeps a wind that is
+ * bilinear in space and linear in time between two frames commented out
+ * (get_wind_vector, kernels.cuh:580-622).  Here both frames live on the
+ * device and icempm_set_forcing_time blends them in one kernel.
+ *
+ * icempm_set_flow_frames: current frames a and b, 2*GridX*GridY doubles each
+ * (vx block, vy block, as icempm_set_current); b NULL repeats a; both NULL
+ * drops the frames (the current set last stays in force). */
+ICEMPM_API int icempm_set_flow_frames(icempm_t *ctx, const double *current_a, const double *current_b);
+
+/* Wind frames on a coarse grid: rows x cols samples of 4 floats {u_a, v_a,
+ * u_b, v_b} (m/s), row-major, row along y and column along x (the reference's
+ * wgrid[lat][lon][4]); sample (r, c) sits at world (x0 + c*cell, y0 + r*cell)
+ * metres.  wind NULL drops the frames (the static wind of the options stays
+ * in force).  Rejects rows or cols < 1, cell <= 0 or non-finite values. */
+ICEMPM_API int icempm_set_wind_frames(icempm_t *ctx, const float *wind, int32_t rows, int32_t cols, double cell,
+                                      double x0, double y0);
+
+/* Blend the frames into the forcing the next sub-steps read: current =
+ * (1-tc)*a + tc*b at every node; with wind frames, wind = (1-tw)*W_a + tw*W_b,
+ * W bilinear at the node's world position (x*cellsize, y*cellsize; clamped
+ * to the wind grid), and wind stress rho_air*C_air*|U|*U (extended forcing).
+ * Weights outside [0, 1] are rejected; ICEMPM_E_STATE when no frames are set.
+ * Asynchronous on the context's stream; under the extended forcing the next
+ * step scatters from the new forcing. */
+ICEMPM_API int icempm_set_forcing_time(icempm_t *ctx, double tc, double tw);
+
+/* The forcing tables the sub-steps read: current (2*GridX*GridY doubles, vx
+ * block then vy block) and the extended forcing's wind stress (same layout,
+ * Pa); either pointer may be NULL.  Synchronises the stream. */
+ICEMPM_API int icempm_get_forcing(icempm_t *ctx, double *current_vxvy, double *wind_stress_xy);
+
 /* Advance `nsteps` sub-steps starting at step index `first_step`.  Step k runs
  * reset_grid, p2g, update_nodes(t = dt*k rounded to float) and
  * g2p(recordPQ = (k % UpdateEveryNthStep == 0)), exactly as the loop in

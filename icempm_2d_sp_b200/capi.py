@@ -25,6 +25,7 @@ EXPORTS = [
     "icempm_mlp_param_count", "icempm_mlp_grad", "icempm_mlp_adam", "icempm_mlp_forward", "icempm_return_map_exact",
     "icempm_return_map_learned", "icempm_harvest_begin", "icempm_harvest_end", "icempm_prepare_frame",
     "icempm_set_flow_frames", "icempm_set_wind_frames", "icempm_set_forcing_time", "icempm_get_forcing",
+    "icempm_download_points_async", "icempm_download_wait",
 ]
 
 FRAME_CHANNELS = ("point_density", "mass", "vx", "vy", "Jpinv", "P", "Q", "r", "g", "b")
@@ -81,6 +82,8 @@ def load(path: str = LIB_PATH):
         "icempm_get_forcing": (C.c_int, [h, dp, dp]),
         "icempm_step": (C.c_int, [h, C.c_int32, C.c_int32]),
         "icempm_download_points": (C.c_int, [h, dp, C.c_uint32, C.POINTER(C.c_uint32)]),
+        "icempm_download_points_async": (C.c_int, [h, dp, C.c_uint32, C.POINTER(C.c_uint32)]),
+        "icempm_download_wait": (C.c_int, [h]),
         "icempm_get_status": (C.c_int, [h, C.POINTER(C.c_uint32), C.POINTER(C.c_int32)]),
         "icempm_clear_force_accumulator": (C.c_int, [h]),
         "icempm_get_boundary_forces": (C.c_int, [h, dp, C.c_int32]),
@@ -275,6 +278,20 @@ class Context:
         check(self._L.icempm_download_points(self.h, _dp(soa), soa.shape[1], C.byref(n)))
         return soa, n.value
 
+    def download_async(self, soa: np.ndarray) -> int:
+        """Start the download into `soa` (keep it alive and unread until
+        download_wait); returns the point count."""
+        if soa.dtype != np.float64 or not soa.flags.c_contiguous or soa.ndim != 2 or soa.shape[0] != N_PTS_ARRAYS:
+            raise ValueError("soa must be a C-contiguous float64 [19, capacity] array")
+        n = C.c_uint32(0)
+        check(self._L.icempm_download_points_async(self.h, _dp(soa), soa.shape[1], C.byref(n)))
+        self._pending = soa
+        return n.value
+
+    def download_wait(self):
+        check(self._L.icempm_download_wait(self.h))
+        self._pending = None
+
     def status(self) -> tuple:
         e, d = C.c_uint32(0), C.c_int32(0)
         check(self._L.icempm_get_status(self.h, C.byref(e), C.byref(d)))
@@ -283,8 +300,13 @@ class Context:
     def clear_force_accumulator(self):
         check(self._L.icempm_clear_force_accumulator(self.h))
 
-    def boundary_forces(self, elapsed_steps: int) -> np.ndarray:
-        out = np.zeros(2 * self.G)
+    def boundary_forces(self, elapsed_steps: int, out: np.ndarray = None) -> np.ndarray:
+        """Boundary forces / (elapsed_steps * dt), fx block then fy block;
+        `out` (2 G doubles, e.g. page-locked) is filled when given."""
+        if out is None:
+            out = np.empty(2 * self.G)
+        elif out.dtype != np.float64 or not out.flags.c_contiguous or out.size != 2 * self.G:
+            raise ValueError(f"out must be a C-contiguous float64 array of {2 * self.G} values")
         check(self._L.icempm_get_boundary_forces(self.h, _dp(out), int(elapsed_steps)))
         return out
 

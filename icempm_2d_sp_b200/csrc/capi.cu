@@ -172,6 +172,19 @@ int icempm_download_points(icempm_t *ctx, double *hssoa, uint32_t capacity, uint
     ICEMPM_TRY(ctx->eng->download(hssoa, capacity, size));
 }
 
+int icempm_download_points_async(icempm_t *ctx, double *hssoa, uint32_t capacity, uint32_t *size)
+{
+    ICEMPM_GUARD_CTX(ctx);
+    if (!hssoa) return fail(ICEMPM_E_ARG, "hssoa is null");
+    ICEMPM_TRY(ctx->eng->download_async(hssoa, capacity, size));
+}
+
+int icempm_download_wait(icempm_t *ctx)
+{
+    ICEMPM_GUARD_CTX(ctx);
+    ICEMPM_TRY(ctx->eng->download_wait());
+}
+
 int icempm_get_status(icempm_t *ctx, uint32_t *error_bits, int32_t *disabled_count)
 {
     ICEMPM_GUARD_CTX(ctx);

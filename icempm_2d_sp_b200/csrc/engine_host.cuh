@@ -280,6 +280,8 @@ public:
         if (n > host_cap) return fail(ICEMPM_E_ARG, "size exceeds the host buffer capacity");
         int rc = ensure_stage();
         if (rc) return rc;
+        rc = stage_free();
+        if (rc) return rc;
         if (n > 0) {
             ICEMPM_CUDA(cudaMemcpy2DAsync(stage_, (size_t)n * sizeof(double), hssoa, (size_t)host_cap * sizeof(double),
                                           (size_t)n * sizeof(double), ICEMPM_N_PTS_ARRAYS, cudaMemcpyHostToDevice, stream_));
@@ -306,18 +308,57 @@ public:
 
     int download(double *hssoa, uint32_t host_cap, uint32_t *size) override
     {
+        int rc = download_async(hssoa, host_cap, size);
+        if (rc) return rc;
+        rc = download_wait();
+        if (rc) return rc;
+        ICEMPM_CUDA(cudaStreamSynchronize(stream_));
+        return 0;
+    }
+
+    // The state is converted into the staging buffer on the compute stream;
+    // the device-to-host copy runs on the copy stream, so sub-steps enqueued
+    // afterwards overlap it.  A later upload or download first waits (on the
+    // device) for the copy that still reads the staging buffer.
+    int download_async(double *hssoa, uint32_t host_cap, uint32_t *size) override
+    {
         if (n_real_ > host_cap) return fail(ICEMPM_E_CAPACITY, "host buffer capacity is smaller than the point count");
         int rc = ensure_stage();
+        if (rc) return rc;
+        if (!copy_stream_) {
+            ICEMPM_CUDA(cudaStreamCreateWithFlags(&copy_stream_, cudaStreamNonBlocking));
+            ICEMPM_CUDA(cudaEventCreateWithFlags(&ev_staged_, cudaEventDisableTiming));
+            ICEMPM_CUDA(cudaEventCreateWithFlags(&ev_copied_, cudaEventDisableTiming));
+        }
+        rc = stage_free();
         if (rc) return rc;
         if (n_ > 0) {
             k_download<Real><<<(n_ + 255) / 256, 256, 0, stream_>>>(pts_[par_], (int)n_, stage_, n_real_);
             ICEMPM_CUDA(cudaGetLastError());
             launches_++;
+            ICEMPM_CUDA(cudaEventRecord(ev_staged_, stream_));
+            ICEMPM_CUDA(cudaStreamWaitEvent(copy_stream_, ev_staged_, 0));
             ICEMPM_CUDA(cudaMemcpy2DAsync(hssoa, (size_t)host_cap * sizeof(double), stage_, (size_t)n_real_ * sizeof(double),
-                                          (size_t)n_real_ * sizeof(double), ICEMPM_N_PTS_ARRAYS, cudaMemcpyDeviceToHost, stream_));
+                                          (size_t)n_real_ * sizeof(double), ICEMPM_N_PTS_ARRAYS, cudaMemcpyDeviceToHost,
+                                          copy_stream_));
+            ICEMPM_CUDA(cudaEventRecord(ev_copied_, copy_stream_));
+            copy_pending_ = true;
         }
-        ICEMPM_CUDA(cudaStreamSynchronize(stream_));
         if (size) *size = n_real_;
+        return 0;
+    }
+    int download_wait() override
+    {
+        if (copy_pending_) {
+            ICEMPM_CUDA(cudaEventSynchronize(ev_copied_));
+            copy_pending_ = false;
+        }
+        return 0;
+    }
+    // the compute stream waits for a copy that still reads the staging buffer
+    int stage_free()
+    {
+        if (copy_pending_) ICEMPM_CUDA(cudaStreamWaitEvent(stream_, ev_copied_, 0));
         return 0;
     }
 
@@ -503,16 +544,18 @@ public:
         return 0;
     }
 
+    // Forces divided by elapsed * dt on the device, into the reference's
+    // [fx block, fy block] layout, then one copy into the caller's buffer.
     int forces(double *fxfy, int elapsed) override
     {
-        std::vector<double2> h(G_);
-        ICEMPM_CUDA(cudaMemcpyAsync(h.data(), force_, G_ * sizeof(double2), cudaMemcpyDeviceToHost, stream_));
-        ICEMPM_CUDA(cudaStreamSynchronize(stream_));
+        if (!force_out_) ICEMPM_CUDA(cudaMalloc(&force_out_, 2 * G_ * sizeof(double)));
         const double div = (double)elapsed * prms_.InitialTimeStep;
-        for (size_t i = 0; i < G_; i++) {
-            fxfy[i] = h[i].x / div;
-            fxfy[G_ + i] = h[i].y / div;
-        }
+        const unsigned nb = (unsigned)((G_ + 255) / 256);
+        k_forces_out<<<nb, 256, 0, stream_>>>(force_, (long long)G_, div, force_out_);
+        ICEMPM_CUDA(cudaGetLastError());
+        launches_++;
+        ICEMPM_CUDA(cudaMemcpyAsync(fxfy, force_out_, 2 * G_ * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+        ICEMPM_CUDA(cudaStreamSynchronize(stream_));
         return 0;
     }
 
@@ -733,6 +776,7 @@ private:
     }
     void release()
     {
+        if (copy_stream_) cudaStreamSynchronize(copy_stream_);
         if (stream_) cudaStreamSynchronize(stream_);
         invalidate_graphs();
         cudaFree(pts_mem_); cudaFree(acc_); cudaFree(vel_); cudaFree(cur_); cudaFree(frc_); cudaFree(status_);
@@ -744,6 +788,11 @@ private:
         for (auto &e : evs_) if (e) cudaEventDestroy(e);
         if (stream_) cudaStreamDestroy(stream_);
         stream_ = nullptr;
+        if (ev_staged_) cudaEventDestroy(ev_staged_);
+        if (ev_copied_) cudaEventDestroy(ev_copied_);
+        if (copy_stream_) cudaStreamDestroy(copy_stream_);
+        copy_stream_ = nullptr;
+        cudaFree(force_out_);
     }
 
     icempm_simparams_t prms_{};
@@ -777,6 +826,10 @@ private:
     double2 *force_ = nullptr;
     DevStatus *st_ = nullptr;
     double *stage_ = nullptr;
+    double *force_out_ = nullptr;          // boundary forces / (elapsed dt), fx block then fy block
+    cudaStream_t copy_stream_ = nullptr;   // device-to-host copies of icempm_download_points_async
+    cudaEvent_t ev_staged_ = nullptr, ev_copied_ = nullptr;
+    bool copy_pending_ = false;
     uint64_t *keys_[2] = {nullptr, nullptr};
     uint32_t *vals_[2] = {nullptr, nullptr};
     uint32_t *runs_ = nullptr;   // padded run starts of the locality order

@@ -20,6 +20,8 @@ public:
     virtual int set_current(const double *cur) = 0;
     virtual int upload(const double *hssoa, uint32_t host_cap, uint32_t n, int32_t disabled) = 0;
     virtual int download(double *hssoa, uint32_t host_cap, uint32_t *size) = 0;
+    virtual int download_async(double *hssoa, uint32_t host_cap, uint32_t *size) = 0;
+    virtual int download_wait() = 0;
     virtual int update_constants(const icempm_simparams_t &p) = 0;
     virtual int step(int nsteps, int first_step) = 0;
     virtual int timings(float ms[4]) = 0;

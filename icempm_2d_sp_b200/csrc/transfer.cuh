@@ -55,6 +55,18 @@ __global__ void k_download(Pts<Real> P, int n, double *__restrict__ stage, size_
     r[18 * pitch] = P.thick64[i];
 }
 
+// Boundary forces per node divided by elapsed steps * dt, into the layout of
+// GPU_Implementation5::grid_boundary_forces (fx block, then fy block).
+static __global__ void __launch_bounds__(256) k_forces_out(const double2 *__restrict__ force, long long G,
+                                                           double div, double *__restrict__ out)
+{
+    const long long i = (long long)blockIdx.x * 256 + threadIdx.x;
+    if (i >= G) return;
+    const double2 f = force[i];
+    out[i] = __ddiv_rn(f.x, div);
+    out[G + i] = __ddiv_rn(f.y, div);
+}
+
 // ---- sorting ---------------------------------------------------------------
 // Locality key: cells grouped in TX x TY tiles, tiles in column order, cells
 // column-major inside a tile; disabled points sort after the enabled ones and

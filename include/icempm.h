@@ -245,6 +245,21 @@ ICEMPM_API int icempm_step(icempm_t *ctx, int32_t nsteps, int32_t first_step);
  * Synchronises the stream.  *size receives the number of points. */
 ICEMPM_API int icempm_download_points(icempm_t *ctx, double *hssoa, uint32_t capacity, uint32_t *size);
 
+/* The same download without waiting for it: the state at this point of the
+ * stream is converted into the context's staging buffer, and its copy into
+ * `hssoa` runs on a second stream, so icempm_step calls made next overlap the
+ * copy (the reference's GPU_Implementation5 carries a
+ * transfer_completion_callback for this purpose, gpu_implementation5.h:45,
+ * unused there).  `hssoa` must stay valid and unread until
+ * icempm_download_wait returns; page-locked memory (icempm_host_register)
+ * lets the copy overlap.  *size receives the number of points at once. */
+ICEMPM_API int icempm_download_points_async(icempm_t *ctx, double *hssoa, uint32_t capacity, uint32_t *size);
+
+/* Wait for the last icempm_download_points_async copy to land in host
+ * memory (sub-steps enqueued after it keep running).  Returns at once when
+ * no copy is outstanding. */
+ICEMPM_API int icempm_download_wait(icempm_t *ctx);
+
 /* Fetch the device error bitmask and disabled-point counter
  * (gpu_partition.cpp:40-48).  Synchronises the stream. */
 ICEMPM_API int icempm_get_status(icempm_t *ctx, uint32_t *error_bits, int32_t *disabled_count);

@@ -1147,6 +1147,9 @@ k_g2p_p2g_batch(const SceneDesc<Real, Acc> *__restrict__ scenes, const int *__re
     extern __shared__ __align__(128) unsigned char smem_raw[];
     SM &sm = *reinterpret_cast<SM *>(smem_raw);
     const int tid = threadIdx.x;
+    // the current scene's descriptor, copied into shared memory when the scene changes
+    __shared__ __align__(16) SceneDesc<Real, Acc> ssd;
+    int cur_scene = -1;
 
     if (tid == 0) {
         mbar_init(&sm.mbar[0], 1);
@@ -1163,7 +1166,17 @@ k_g2p_p2g_batch(const SceneDesc<Real, Acc> *__restrict__ scenes, const int *__re
     const bool store_vc = step == bst->vc_step;
 
     for (int it = 0; c < nchunks; it++, c += (int)gridDim.x) {
-        const SceneDesc<Real, Acc> &S = scenes[chunk_scene[c]];
+        const int sc = chunk_scene[c];
+        if (sc != cur_scene) {   // block-uniform: every thread of the CTA walks the same chunks
+            __syncthreads();
+            static_assert(sizeof(SceneDesc<Real, Acc>) % 4 == 0, "word copy");
+            const uint32_t *src = reinterpret_cast<const uint32_t *>(&scenes[sc]);
+            uint32_t *dst = reinterpret_cast<uint32_t *>(&ssd);
+            for (int k = tid; k < (int)(sizeof(SceneDesc<Real, Acc>) / 4); k += BT) dst[k] = src[k];
+            __syncthreads();
+            cur_scene = sc;
+        }
+        const SceneDesc<Real, Acc> &S = ssd;
         const int s = STAGES == 2 ? (it & 1) : 0;
         const uint32_t parity = STAGES == 2 ? ((uint32_t)(it >> 1) & 1u) : ((uint32_t)it & 1u);
         uint32_t err = 0, perr = 0;

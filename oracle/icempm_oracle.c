@@ -535,7 +535,7 @@ uint32_t orc_g2p(const SP *p, double *soa, size_t pitch, size_t n, const double 
     uint32_t err = 0;
     int32_t ndis = 0;
     const double h_inv = p->cellsize_inv, dt = p->InitialTimeStep;
-    const double mu = p->mu, kappa = p->kappa;
+    const double mu = p->mu;
     const int gridY = p->GridYTotal, gridX = p->GridXTotal;
     const long long nnodes = (long long)gridX * gridY;
 #pragma omp parallel for schedule(static) reduction(| : err) reduction(+ : ndis)

@@ -209,8 +209,17 @@ template <> struct AccOps<long long> {
     static __device__ __forceinline__ long long cvt(double v) { return __double2ll_rn(v); }
     template <class Real>
     static __device__ __forceinline__ Real to(long long v, double inv_scale) { return Real(double(v) * inv_scale); }
+    // A 64-bit shared-memory atomic add is a compare-and-swap loop on sm_100a;
+    // two native 32-bit adds give the same sum modulo 2^64: the low words add
+    // with a returned old value, and each addition that wraps the low word
+    // carries one into the high word.  The total carry is the same in every
+    // order, so the tile sum stays exact and order-independent.
     static __device__ __forceinline__ void add_shared(long long *a, long long v) {
-        atomicAdd(reinterpret_cast<unsigned long long *>(a), (unsigned long long)v);
+        unsigned *w = reinterpret_cast<unsigned *>(a);       // w[0] low word, w[1] high word
+        const unsigned lo = (unsigned)(unsigned long long)v;
+        const unsigned hi = (unsigned)((unsigned long long)v >> 32);
+        const unsigned old = atomicAdd(w, lo);
+        atomicAdd(w + 1, hi + ((old + lo < old) ? 1u : 0u));
     }
     static __device__ __forceinline__ void add_global(long long *a, long long v) { red_global_add(a, v); }
 };

@@ -52,8 +52,8 @@ B_POINT, B_NODE = 124, 49
 # flushes 12 B of accumulators per node; the grid update moves the other 29 B
 B_NODE_FUSED = 20
 # measured DRAM traffic of the fused kernel per point, grid share included
-# (489.08 MB for 5,884,928 points and 2,097,152 nodes in one launch)
-TRAFFIC_B_PER_POINT = 83.11
+# (489.86 MB for 5,884,928 points and 2,097,152 nodes in one launch)
+TRAFFIC_B_PER_POINT = 83.24
 
 
 def parse():

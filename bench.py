@@ -42,7 +42,7 @@ sys.path.insert(0, ROOT)
 
 METRIC = "particle-steps/s on 1 B200, chosen vs plain at ≤1e-4 err vs FP64; % HBM peak"
 UNIT = "particle-steps/s"
-WORKLOAD = ("config1: plain MPM at scale, 4096x2048 grid, h=1 m, 2000 Voronoi floes (70% kept), "
+WORKLOAD = ("floe field: plain MPM at scale, 4096x2048 grid, h=1 m, 2000 Voronoi floes (70% kept), "
             "4 ppc +-0.25h jitter, lognormal(0,0.3) thickness, Rankine wind 20 m/s @ 800 cells, dt=1e-4 s")
 FALLBACK_HBM_GBS = 6650.0
 # algorithmic bytes per step: 124 per point + 49 per grid node (FP32/u32 words,
@@ -62,8 +62,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["config1", "ensemble"], default="config1",
-                    help="ensemble: the batched config-3 workload (96 scenes, one launch per kernel per sub-step)")
+    ap.add_argument("--workload", choices=["floe_field", "ensemble"], default="floe_field",
+                    help="ensemble: 96 independent scenes of 10k-2M points in one batch (one launch per kernel per sub-step)")
     ap.add_argument("--ensemble-scenes", type=int, default=96)
     ap.add_argument("--max-points", type=int, default=None,
                     help="keep whole floes until this many points (the ~8.4M-point variant)")
@@ -141,11 +141,11 @@ class ClockSampler:
 def make_scene(seed, max_points=None, sample=False, grid=None):
     from icempm_2d_sp_b200 import scenes
     if sample:  # the same generation rules on a 1024x512 sub-domain (1/16 of the cells)
-        return scenes.config1(seed=seed, gx=1024, gy=512, n_seeds=125)
+        return scenes.floe_field(seed=seed, gx=1024, gy=512, n_seeds=125)
     if grid is not None:
         gx, gy = grid
-        return scenes.config1(seed=seed, gx=gx, gy=gy, n_seeds=max(1, round(2000 * gx * gy / (4096 * 2048))))
-    return scenes.config1(seed=seed, max_points=max_points)
+        return scenes.floe_field(seed=seed, gx=gx, gy=gy, n_seeds=max(1, round(2000 * gx * gy / (4096 * 2048))))
+    return scenes.floe_field(seed=seed, max_points=max_points)
 
 
 def run_reference(args, rank):
@@ -156,7 +156,7 @@ def run_reference(args, rank):
     sc = make_scene(1235, sample=True)
     grid = np.zeros((9, sc.grid_nodes))
     grid[5], grid[6] = sc.current[:sc.grid_nodes], sc.current[sc.grid_nodes:]
-    sample = (f"config1 generation rules on a 1024x512 sub-domain (125 seeds), N={sc.n} points, "
+    sample = (f"floe-field generation rules on a 1024x512 sub-domain (125 seeds), N={sc.n} points, "
               f"one sub-step per step")
     try:
         from oracle.refbuild import build_ref
@@ -215,7 +215,7 @@ def reference_gpu_baseline(args, sc):
 
 
 def run_ensemble(args, rank, world, local, dist):
-    """independent scenes (point counts log-uniform in
+    """The ensemble workload: independent scenes (point counts log-uniform in
     10k-2M, Voronoi floes, grids 128x128 to 2048x1024, uniform wind 5-25 m/s
     and current 0-0.3 m/s) advanced by one batched launch of each kernel per
     sub-step in CUDA graphs of 50, kernel shape and sort cadence from the
@@ -263,8 +263,8 @@ def run_ensemble(args, rank, world, local, dist):
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-                "data": "synthetic (seeded scene generator, BASELINE config 3 rules)",
-                "config": {"workload": f"config3: {args.ensemble_scenes} scenes, 10k-2M points log-uniform, "
+                "data": "synthetic (seeded ensemble generator: Voronoi floe fields of 10k-2M points)",
+                "config": {"workload": f"ensemble: {args.ensemble_scenes} scenes, 10k-2M points log-uniform, "
                                        "Voronoi floes, grids 128x128..2048x1024, uniform wind 5-25 m/s, "
                                        "current 0-0.3 m/s", "points": int(n), "points_all_ranks": n_tot,
                            "scenes_this_rank": len(scs), "grid_nodes": G,
@@ -397,7 +397,7 @@ def main():
     fused_launch_s = fused * 1e-3 / args.steps
     achieved = fused_bytes / fused_launch_s / 1e9
     # DRAM bytes of one fused launch from an ncu capture (dram__bytes_read.sum +
-    # dram__bytes_write.sum of profiles/k_g2p_p2g_config1_2048x1024.md), per
+    # dram__bytes_write.sum of profiles/k_g2p_p2g_floe_field_2048x1024.md), per
     # point, scaled to this scene's point count (same node/point ratio)
     traffic = TRAFFIC_B_PER_POINT * n
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
@@ -424,7 +424,7 @@ def main():
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-                "data": "synthetic (seeded scene generator, BASELINE config 1 rules)",
+                "data": "synthetic (seeded Voronoi floe-field generator)",
                 "config": {"workload": workload, "points": int(n), "points_all_ranks": n_tot, "grid_nodes": G,
                            "variant": "fixed: int64 fixed-point P2G, FP32 state (chosen form)",
                            "forcing": "extended (Rankine wind, quadratic water drag)",

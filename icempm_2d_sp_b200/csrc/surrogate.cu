@@ -1,4 +1,4 @@
-// surrogate.cu -- the learned return map.
+// surrogate.cu -- the learned return map (an MLP in place of the Drucker-Prager projection).
 //
 // An MLP 4 -> 64 -> 64 -> 3 with SiLU stands in for the projection of a
 // trial state onto the Drucker-Prager yield surface (case 3 of wolper_dp,

@@ -6,11 +6,11 @@ These generators produce the same artefacts -- SimParams, the grid status
 bytes (100 = modelled water, 0 = land/wall), the current field and an HSSOA in
 the reference layout -- from a seed, for the benchmark scene families:
 
-  config0   256x128 grid, h=2 m, 200x80-cell rectangle at 2x2 ppc (64,000 points)
-  config1   4096x2048 grid, h=1 m, 2000 Voronoi floes (70% kept), 4 ppc,
-            lognormal(0, 0.3) thickness per floe, Rankine-vortex wind
-  ridging   1024x512 grid, h=2 m, ~1M crushed points driven at 2 m/s against x=0
-  random    small grids with randomised state, for parity tests
+  ice_block   256x128 grid, h=2 m, 200x80-cell rectangle at 2x2 ppc (64,000 points)
+  floe_field  4096x2048 grid, h=1 m, 2000 Voronoi floes (70% kept), 4 ppc,
+              lognormal(0, 0.3) thickness per floe, Rankine-vortex wind (23.0M points)
+  ridging     1024x512 grid, h=2 m, ~1M crushed points driven at 2 m/s against x=0
+  random      small grids with randomised state, for parity tests
 
 Particles sit on a 2x2 lattice per cell (sub-cell centres) with uniform jitter
 of +-0.25h, then go through the reference's integer-cell conversion
@@ -117,7 +117,7 @@ def _sort_by_cell(x, y, h, gy, *extra):
     return (x[order], y[order]) + tuple(e[order] for e in extra)
 
 
-def config0(seed=1234, forcing=FORCING_COMPAT) -> Scene:
+def ice_block(seed=1234, forcing=FORCING_COMPAT) -> Scene:
     """256x128 grid, h=2 m, 200x80-cell ice rectangle, 2x2 ppc, jitter +-0.25h
     (64,000 points), thickness 1 m, zero velocity, current 0.1 m/s along +x,
     dt=2e-4 s, 1000 steps.  Extended forcing adds a uniform 10 m/s wind along +x."""
@@ -133,7 +133,7 @@ def config0(seed=1234, forcing=FORCING_COMPAT) -> Scene:
     opts = Options.default(forcing=forcing)
     if forcing == FORCING_EXTENDED:
         opts.wind_kind, opts.wind_u, opts.wind_v = WIND_UNIFORM, 10.0, 0.0
-    return Scene("config0", p, wall_ring_status(gx, gy), uniform_current(gx, gy, 0.1),
+    return Scene("ice_block", p, wall_ring_status(gx, gy), uniform_current(gx, gy, 0.1),
                  soa, len(x), 1000, opts, seed)
 
 
@@ -157,7 +157,7 @@ def voronoi_floes(gx, gy, n_seeds, keep, rng, margin=3):
     return floe, cx, cy, seeds
 
 
-def config1(seed=1235, gx=4096, gy=2048, n_seeds=2000, keep=0.7, forcing=FORCING_EXTENDED,
+def floe_field(seed=1235, gx=4096, gy=2048, n_seeds=2000, keep=0.7, forcing=FORCING_EXTENDED,
             max_points=None) -> Scene:
     """4096x2048 grid, h=1 m; 2000 Voronoi floes with 70% kept; 4 ppc with
     +-0.25h jitter; per-floe thickness lognormal(0, 0.3) m; Rankine-vortex wind
@@ -188,7 +188,7 @@ def config1(seed=1235, gx=4096, gy=2048, n_seeds=2000, keep=0.7, forcing=FORCING
     opts.wind_kind = WIND_RANKINE
     opts.wind_cx, opts.wind_cy = centre[0] * h, centre[1] * h
     opts.wind_vmax, opts.wind_radius = 20.0, 800.0 * h
-    return Scene("config1", p, wall_ring_status(gx, gy), uniform_current(gx, gy, 0.1),
+    return Scene("floe_field", p, wall_ring_status(gx, gy), uniform_current(gx, gy, 0.1),
                  soa, len(x), 200, opts, seed,
                  info={"floes_kept": int(len(np.unique(floe[ice]))), "n_seeds": n_seeds})
 
@@ -200,7 +200,7 @@ ENSEMBLE_GRIDS = [(128, 128), (256, 128), (256, 256), (512, 256), (512, 512), (1
 
 def ensemble_scene(seed, target_points, wind_speed, wind_dir, current_speed, current_dir,
                    forcing=FORCING_EXTENDED) -> Scene:
-    """One scene of the batched-ensemble workload: config-1 generation rules
+    """One scene of the batched-ensemble workload: floe-field generation rules
     (Voronoi floes, 70% kept, 4 ppc, lognormal thickness) on the smallest grid
     of ENSEMBLE_GRIDS that holds `target_points`, whole floes kept up to that
     count; uniform wind and current of the given speeds and directions."""
@@ -210,7 +210,7 @@ def ensemble_scene(seed, target_points, wind_speed, wind_dir, current_speed, cur
             gx, gy = g
             break
     n_seeds = max(8, round(gx * gy / 1500))   # floes of ~1500 cells, so whole floes approach the target
-    sc = config1(seed=seed, gx=gx, gy=gy, n_seeds=n_seeds, forcing=forcing, max_points=target_points)
+    sc = floe_field(seed=seed, gx=gx, gy=gy, n_seeds=n_seeds, forcing=forcing, max_points=target_points)
     sc.options.wind_kind = WIND_UNIFORM
     sc.options.wind_u = float(wind_speed * np.cos(wind_dir))
     sc.options.wind_v = float(wind_speed * np.sin(wind_dir))
@@ -223,9 +223,9 @@ def ensemble_scene(seed, target_points, wind_speed, wind_dir, current_speed, cur
 
 
 def ensemble(n_scenes=96, seed=4242, n_min=10_000, n_max=2_000_000, forcing=FORCING_EXTENDED):
-    """Batched-ensemble workload (BASELINE config 3): `n_scenes` independent
+    """Batched-ensemble workload: `n_scenes` independent
     scenes, point counts log-uniform in [n_min, n_max], Voronoi floes as in
-    config 1, grids from 128x128 to 2048x1024 sized to each scene, wind speed
+    the floe field, grids from 128x128 to 2048x1024 sized to each scene, wind speed
     uniform in 5-25 m/s with a uniform direction, current uniform in
     0-0.3 m/s with a uniform direction."""
     return [ensemble_scene(**spec, forcing=forcing) for spec in ensemble_specs(n_scenes, seed, n_min, n_max)]
@@ -314,4 +314,4 @@ def random_state(seed=7, gx=64, gy=48, h=1.5, dt=1e-4, fill=0.6, ppc_side=2, str
     return Scene("random", p, wall_ring_status(gx, gy), cur, soa, n, 10, opts, seed)
 
 
-BUILDERS = {"config0": config0, "config1": config1, "ridging": ridging, "random": random_state}
+BUILDERS = {"ice_block": ice_block, "floe_field": floe_field, "ridging": ridging, "random": random_state}

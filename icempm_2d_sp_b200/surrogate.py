@@ -1,4 +1,4 @@
-"""Host side of the learned return map.
+"""Host side of the learned return map (an MLP in place of the Drucker-Prager projection).
 
 Data: (trial, projected) pairs recorded by the fused kernel
 (`Context.harvest_begin/harvest_end`, 8 floats per record).  Training runs on

@@ -353,7 +353,7 @@ typedef struct icempm_frame_t {
 ICEMPM_API int icempm_prepare_frame(icempm_t *ctx, const uint32_t *point_colors_rgb, uint32_t ncolors,
                                     int32_t elapsed_steps, icempm_frame_t *out);
 
-/* ---- Ensembles (no counterpart in the reference) --------
+/* ---- Ensembles (many scenes per launch; no counterpart in the reference) ---
  * Many independent scenes advanced together: one launch of the grid update
  * and one of the fused kernel per sub-step cover every scene of the batch,
  * captured in CUDA graphs.  Each scene is an ordinary context (created,
@@ -387,7 +387,7 @@ ICEMPM_API int icempm_batch_get_tuning(icempm_batch_t *batch, icempm_batch_tunin
 ICEMPM_API int icempm_batch_timings(icempm_batch_t *batch, float ms[4]);
 ICEMPM_API int icempm_batch_launch_count(icempm_batch_t *batch, uint64_t *count);
 
-/* ---- Learned return map (no counterpart in the reference)
+/* ---- Learned return map (no counterpart in the reference) -----------------
  * An MLP 4 -> 64 -> 64 -> 3 (SiLU) that stands in for the projection of a
  * trial state onto the Drucker-Prager yield surface (wolper_dp's case 3,
  * kernels.cuh:411-467).  A trial state is 4 floats (sigma1 >= sigma2 of Fe,

@@ -11,7 +11,7 @@ with nvcc's default floating-point flags (its CMakeLists.txt leaves
 CMAKE_CUDA_FLAGS at the default); so does this recipe, for sm_100a instead of
 its "80;89".  Needs the reference checkout, so it runs only where the checkout
 exists; the built library travels with the repository snapshot.  TEST AND
-BASELINE INFRASTRUCTURE ONLY.
+MEASUREMENT INFRASTRUCTURE ONLY.
 """
 import ctypes as C
 import os

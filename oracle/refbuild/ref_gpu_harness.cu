@@ -12,7 +12,7 @@
  * with the sub-step loop of Model::Step (simulation/model.cpp:18-39):
  * simulation time passed as float, recordPQ when step % UpdateEveryNthStep == 0.
  * One scene at a time (the reference keeps its state in __constant__ /
- * __device__ symbols).  TEST AND BASELINE INFRASTRUCTURE ONLY: it measures
+ * __device__ symbols).  TEST AND MEASUREMENT INFRASTRUCTURE ONLY: it measures
  * the reference's GPU step and pins parity against it; the product never
  * links it. */
 #include <cstddef>

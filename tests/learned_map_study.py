@@ -1,8 +1,8 @@
-"""Learned return map study.
+"""Learned return map study (16M-point ridging scene, 8192x2048 grid).
 
 1. Training pairs: projections recorded by the fused kernel from plain-method
    runs -- the 1M-point ridging scene (1024x512 grid, 2 m/s against the wall)
-   and the config-1 scene on a 2048x1024 grid -- up to --pairs records.
+   and the floe-field scene on a 2048x1024 grid -- up to --pairs records.
 2. Training: the library's GPU kernels (icempm_mlp_grad + icempm_mlp_adam),
    minibatch Adam on standardised features.
 3. Evaluation: trial states recorded from a 16M-point compressive ridging
@@ -57,10 +57,10 @@ def main():
     r1, o1 = harvest(scenes.ridging(), 1000, a.pairs, 2)
     parts = [r1]
     if len(r1) < a.pairs:
-        sc1 = scenes.config1(gx=2048, gy=1024, n_seeds=500)
+        sc1 = scenes.floe_field(gx=2048, gy=1024, n_seeds=500)
         r2, o2 = harvest(sc1, 200, a.pairs - len(r1), 1)
         parts.append(r2)
-        out["pairs_config1"] = int(len(r2))
+        out["pairs_floe_field"] = int(len(r2))
     rec = np.concatenate(parts)
     out["pairs"] = int(len(rec))
     out["pairs_ridging"] = int(len(r1))

@@ -1,7 +1,7 @@
-"""Precision study (BASELINE config 2): the GPU step's variants against the
+"""Precision study: the GPU step's variants against the
 FP64 CPU oracle.
 
-Scenes: config 0 (64,000 points, 10 m/s wind, current 0.1 m/s) and the
+Scenes: the ice block (64,000 points, 10 m/s wind, current 0.1 m/s) and the
 ridging scene (1024x512 grid, 1M points driven at 2 m/s against the x=0 wall,
 all points crushed, so the Drucker-Prager return map acts on every point).
 Each runs 1, 100 and 1000 sub-steps from its initial state in three
@@ -16,7 +16,7 @@ oracle at the same step:
   mass                relative difference of the total mass of enabled points
   flags               points whose utility word (crushed / disabled) differs
 
-    python tests/precision_study.py [--scenes config0,ridging] [--steps 1,100,1000] [--json out.json]
+    python tests/precision_study.py [--scenes ice_block,ridging] [--steps 1,100,1000] [--json out.json]
 
 The oracle is test infrastructure; this script is a checker, never on the
 product path.
@@ -41,8 +41,8 @@ VARIANTS = ["fp32", "fixed", "fp64"]
 
 
 def make(name):
-    if name == "config0":
-        return scenes.config0(forcing=FORCING_EXTENDED)
+    if name == "ice_block":
+        return scenes.ice_block(forcing=FORCING_EXTENDED)
     if name == "ridging":
         return scenes.ridging()
     raise ValueError(name)
@@ -138,7 +138,7 @@ def table(rows):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--scenes", default="config0,ridging")
+    ap.add_argument("--scenes", default="ice_block,ridging")
     ap.add_argument("--steps", default="1,100,1000")
     ap.add_argument("--json", default=None)
     a = ap.parse_args()

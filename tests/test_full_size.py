@@ -1,7 +1,7 @@
 """Parity at the benchmark's full sizes.
 
-Config 1 (4096x2048 grid, 23.0M points, Voronoi floes, Rankine wind,
-extended forcing) and the config-4-sized compressive ridging scene (8192x2048
+The floe field (4096x2048 grid, 23.0M points, Voronoi floes, Rankine wind,
+extended forcing) and a 16M-point compressive ridging scene (8192x2048
 grid, 16.0M points, every point crushed so the return map runs) are advanced
 10 sub-steps by the chosen form (fixed-point P2G, FP32 state) and by the FP64
 oracle on the host cores, on the same seeded inputs.
@@ -49,11 +49,11 @@ def _digest(soa, n):
     return hashlib.sha256(np.ascontiguousarray(soa[:, :n]).tobytes()).hexdigest()
 
 
-@pytest.mark.parametrize("which", ["config1", "ridging_16M"])
+@pytest.mark.parametrize("which", ["floe_field_23M", "ridging_16M"])
 def test_full_size_against_fp64_oracle(capi, which):
     import oracle
-    if which == "config1":
-        sc = scenes.config1()
+    if which == "floe_field_23M":
+        sc = scenes.floe_field()
     else:
         sc = scenes.ridging(gx=8192, gy=2048, cells_x=4000, cells_y=1000, h=1.0, dt=1e-4, speed=2.0)
     opts = Options.default()

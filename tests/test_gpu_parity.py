@@ -239,8 +239,8 @@ def test_1000_steps_aggregates(capi, variant):
 
 
 @pytest.mark.slow
-def test_config0_1000_steps(capi):
-    sc = scenes.config0()
+def test_ice_block_1000_steps(capi):
+    sc = scenes.ice_block()
     ref, _, rerr, _ = _oracle_run(sc, 1000)
     out, err, dis = run_gpu(capi, sc.prms, sc.status, sc.current, sc.soa, sc.n, 1000, 0, "fixed")
     a, b = aggregates(out, sc.n, sc.prms), aggregates(ref, sc.n, sc.prms)

@@ -63,7 +63,7 @@ def test_reset_defaults_match_reference(ref_lib):
 
 
 def test_compute_helpers_match_reference(ref_lib):
-    sc = scenes.config0()
+    sc = scenes.ice_block()
     a = sc.prms.copy()
     ref_lib.ref_compute_helpers(C.byref(a))
     b = sc.prms.copy()
@@ -164,7 +164,7 @@ def test_svd_reconstruction_and_conventions():
 
 
 def test_kirchhoff_and_pq_consistency():
-    p = scenes.config0().prms
+    p = scenes.ice_block().prms
     F = np.array([[1.001, 2e-4], [-1e-4, 0.998]])
     tau = oracle.kirchhoff(p, F)
     Je, pp, q = oracle.compute_pq(p, F)
@@ -184,7 +184,7 @@ def _dp_inputs(p, F):
 
 
 def test_return_map_cases():
-    p = scenes.config0().prms
+    p = scenes.ice_block().prms
     # case 0/1: tension (p < DP_threshold_p)
     F = np.diag([1.001, 1.001])
     Je, pp, q, U, V, sig2, shat = _dp_inputs(p, F)
@@ -215,7 +215,7 @@ def test_return_map_cases():
 
 
 def test_failure_surface_latch():
-    p = scenes.config0().prms
+    p = scenes.ice_block().prms
     assert oracle.failure_check(p, 0, -2e7, 0) & STATUS_CRUSHED          # below pmin2
     assert not oracle.failure_check(p, 0, 1e5, 1e3) & STATUS_CRUSHED     # deep inside
     assert oracle.failure_check(p, 0, 1e5, 5e6) & STATUS_CRUSHED         # shear beyond ellipse

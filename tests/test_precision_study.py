@@ -1,5 +1,5 @@
-"""The precision study's machinery on the small scene (config 0, 64,000
-points, wind), against the FP64 oracle.  The full study (config 0 and the
+"""The precision study's machinery on the small scene (the ice block, 64,000
+points, wind), against the FP64 oracle.  The full study (the ice block and the
 1M-point ridging scene at 1, 100 and 1000 steps) is tests/precision_study.py.
 
 Tolerances: FP64 on the GPU within 1e-9 cells and 1e-9 relative velocity;
@@ -14,12 +14,12 @@ import precision_study as ps
 pytestmark = pytest.mark.gpu
 
 
-def test_precision_study_config0_short():
+def test_precision_study_ice_block_short():
     from icempm_2d_sp_b200 import capi
     capi.load()
     if capi.device_count() < 1:
         pytest.fail("no CUDA device visible to the library")
-    rows = ps.run(["config0"], [1, 20])
+    rows = ps.run(["ice_block"], [1, 20])
     assert len(rows) == 6
     for r in rows:
         assert r["device_errors"] == 0 and r["mass"] == 0.0 and r["flags"] == 0, r

@@ -71,9 +71,9 @@ def test_reference_gpu_step_matches_golden(ref_gpu, name):
 
 @pytest.fixture(scope="module")
 def voronoi_scene():
-    # config1 generation rules on a 256x128 grid (76k points); the reference
+    # floe-field generation rules on a 256x128 grid (76k points); the reference
     # has no wind term, so both sides run the reference's forcing
-    return scenes.config1(seed=77, gx=256, gy=128, n_seeds=8)
+    return scenes.floe_field(seed=77, gx=256, gy=128, n_seeds=8)
 
 
 @pytest.mark.parametrize("nsteps", [1, 20])

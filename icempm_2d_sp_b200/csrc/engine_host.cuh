@@ -722,7 +722,7 @@ public:
                                   2 * ICEMPM_MAX_REGIONS * sizeof(float);
         ICEMPM_CUDA(cudaMemsetAsync(frame_mem_, 0, zero_bytes, stream_));
         if (n_ > 0) {
-            k_frame_scatter<Real><<<(n_ + 255) / 256, 256, 0, stream_>>>(
+            k_frame_scatter<Real><<<(n_ + 1023) / 1024, 256, 0, stream_>>>(
                 pts_[par_], (int)n_, gx_, gy_, Real(prms_.ParticleMass), (colors && ncolors) ? colors_ : nullptr,
                 (colors && ncolors) ? ncolors : 0u, frame_);
             launches_++;

@@ -11,9 +11,10 @@
 // reaction of each node, divided by elapsed steps * dt, is summed per region
 // (status >= 100 -> status - 99, else status).
 //
-// k_frame_scatter: one point per thread over the locality-sorted points; a
-// CTA's nodes are accumulated in a shared tile (FP32 shared atomics) and
-// flushed with one global atomic per non-zero node and channel.
+// k_frame_scatter: four entries of the locality order per thread (one cell,
+// as the sort arranged them), summed in registers per node; a CTA's nodes are
+// accumulated in a shared tile (FP32 shared atomics) and flushed with one
+// global atomic per non-zero node and channel.
 // k_frame_finish: one node per thread; region sums reduced in shared memory.
 #pragma once
 #include "engine.cuh"
@@ -32,6 +33,44 @@ struct FrameOut {
     float *region_force;         // 2 * ICEMPM_MAX_REGIONS
 };
 
+// Channel values of one point: density weight, mass, m vx, m vy, Jp_inv, P, Q, r, g, b.
+template <class Real>
+__device__ __forceinline__ void frame_values(const Pts<Real> &P, int i, Real particle_mass,
+                                             const uint32_t *__restrict__ colors, uint32_t ncolors,
+                                             float vals[kFrameChannels], float &x, float &y)
+{
+    const V4<Real> A = P.A[i];
+    const V2<Real> v = P.V[i], pq = P.PQ[i];
+    const uint32_t pid = P.pid[i];
+    const uint32_t col = (colors && pid < ncolors) ? colors[pid] : 0xffffffu;
+    const float mp = float(particle_mass * A.w);
+    vals[0] = 1.0f; vals[1] = mp; vals[2] = mp * float(v.x); vals[3] = mp * float(v.y);
+    vals[4] = float(A.z); vals[5] = float(pq.x); vals[6] = float(pq.y);
+    vals[7] = float((col >> 16) & 0xff); vals[8] = float((col >> 8) & 0xff); vals[9] = float(col & 0xff);
+    x = float(A.x); y = float(A.y);
+}
+
+// Adds node (X, Y)'s channel sums into the CTA tile, or into the grid when
+// the tile is off.
+__device__ __forceinline__ void frame_node_add(float (*tile)[kFrameTile], bool on, int x0, int y0, int th,
+                                               const FrameOut &F, int gy, int X, int Y, const float add[kFrameChannels])
+{
+    if (on) {
+        const int li = (X - x0) * th + (Y - y0);
+#pragma unroll
+        for (int c = 0; c < kFrameChannels; c++) atomicAdd(&tile[c][li], add[c]);
+    } else {
+        const size_t node = (size_t)X * gy + Y;
+#pragma unroll
+        for (int c = 0; c < kFrameChannels; c++) atomicAdd(&F.ch[c][node], add[c]);
+    }
+}
+
+// A CTA takes 1024 entries of the locality order: 8 warps x 128, thread
+// (warp w, lane l) the entries w*128 + 32j + l, j = 0..3, which the sort put
+// in one cell.  When a thread's enabled points do share a cell, their node
+// terms are summed in registers first (one shared atomic per node and
+// channel for up to four points); otherwise each point adds its own.
 template <class Real>
 __global__ void __launch_bounds__(256) k_frame_scatter(Pts<Real> P, int n, int gx, int gy, Real particle_mass,
                                                        const uint32_t *__restrict__ colors, uint32_t ncolors,
@@ -41,23 +80,33 @@ __global__ void __launch_bounds__(256) k_frame_scatter(Pts<Real> P, int n, int g
     __shared__ int box[4];
     if (threadIdx.x == 0) { box[0] = INT_MAX; box[1] = INT_MAX; box[2] = -1; box[3] = -1; }
     __syncthreads();
-    const int i = blockIdx.x * 256 + threadIdx.x;
-    bool active = false;
-    int cx = 0, cy = 0;
-    uint2 key = make_uint2(0u, kDisabled);
-    if (i < n) {
-        key = P.K[i];
-        cx = (int)(key.x & 0xffff); cy = (int)(key.x >> 16);
-        active = !(key.y & kDisabled) && cx >= 1 && cx <= gx - 2 && cy >= 1 && cy <= gy - 2;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int e0 = blockIdx.x * 1024 + w * 128 + lane;
+    bool act[4];
+    int cxs[4], cys[4];
+    unsigned xmn = 0x7fffffffu, ymn = 0x7fffffffu, xmx = 0u, ymx = 0u;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        const int i = e0 + 32 * j;
+        act[j] = false; cxs[j] = 0; cys[j] = 0;
+        if (i < n) {
+            const uint2 key = P.K[i];
+            const int cx = (int)(key.x & 0xffff), cy = (int)(key.x >> 16);
+            act[j] = !(key.y & kDisabled) && cx >= 1 && cx <= gx - 2 && cy >= 1 && cy <= gy - 2;
+            cxs[j] = cx; cys[j] = cy;
+            if (act[j]) {
+                xmn = min(xmn, (unsigned)cx); ymn = min(ymn, (unsigned)cy);
+                xmx = max(xmx, (unsigned)cx); ymx = max(ymx, (unsigned)cy);
+            }
+        }
     }
     {
         const unsigned FULL = 0xffffffffu;
-        const unsigned xmn = __reduce_min_sync(FULL, active ? (unsigned)cx : 0x7fffffffu);
-        const unsigned ymn = __reduce_min_sync(FULL, active ? (unsigned)cy : 0x7fffffffu);
-        const unsigned xmx = __reduce_max_sync(FULL, active ? (unsigned)cx : 0u);
-        const unsigned ymx = __reduce_max_sync(FULL, active ? (unsigned)cy : 0u);
-        const bool warp_any = __any_sync(FULL, active);   // every lane votes (a skipped lane stalls the warp)
-        if ((threadIdx.x & 31) == 0 && warp_any) {
+        xmn = __reduce_min_sync(FULL, xmn); ymn = __reduce_min_sync(FULL, ymn);
+        xmx = __reduce_max_sync(FULL, xmx); ymx = __reduce_max_sync(FULL, ymx);
+        const bool any = act[0] || act[1] || act[2] || act[3];
+        const bool warp_any = __any_sync(FULL, any);   // every lane votes (a skipped lane stalls the warp)
+        if (lane == 0 && warp_any) {
             atomicMin(&box[0], (int)xmn); atomicMin(&box[1], (int)ymn);
             atomicMax(&box[2], (int)xmx); atomicMax(&box[3], (int)ymx);
         }
@@ -71,38 +120,68 @@ __global__ void __launch_bounds__(256) k_frame_scatter(Pts<Real> P, int n, int g
 #pragma unroll
         for (int c = 0; c < kFrameChannels; c++) tile[c][k] = 0.0f;
     __syncthreads();
-    if (active) {
-        const V4<Real> A = P.A[i];
-        const V2<Real> v = P.V[i], pq = P.PQ[i];
-        const uint32_t pid = P.pid[i];
-        const uint32_t col = (colors && pid < ncolors) ? colors[pid] : 0xffffffu;
-        const float vals[kFrameChannels] = {1.0f, 0.0f, 0.0f, 0.0f, float(A.z), float(pq.x), float(pq.y),
-                                            float((col >> 16) & 0xff), float((col >> 8) & 0xff), float(col & 0xff)};
-        const float mp = float(particle_mass * A.w);
-        Real wx[3], wy[3];
-        bspline(A.x, wx);
-        bspline(A.y, wy);
+
+    // the thread's enabled points: one cell?
+    int first = -1, nact = 0;
+    bool one_cell = true;
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+        if (act[j]) {
+            if (first < 0) first = j;
+            else if (cxs[j] != cxs[first] || cys[j] != cys[first]) one_cell = false;
+            nact++;
+        }
+    if (nact > 0 && one_cell) {
+        float vals[4][kFrameChannels], wx[4][3], wy[4][3];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            float x = 0.0f, y = 0.0f;
+            if (act[j]) {
+                frame_values(P, e0 + 32 * j, particle_mass, colors, ncolors, vals[j], x, y);
+                bspline(x, wx[j]);
+                bspline(y, wy[j]);
+            } else {
+#pragma unroll
+                for (int c = 0; c < kFrameChannels; c++) vals[j][c] = 0.0f;
+#pragma unroll
+                for (int k = 0; k < 3; k++) { wx[j][k] = 0.0f; wy[j][k] = 0.0f; }
+            }
+        }
+        int cx = 0, cy = 0;
+#pragma unroll
+        for (int j = 0; j < 4; j++) if (j == first || (first < 0 && j == 0)) { cx = cxs[j]; cy = cys[j]; }
         for (int a = 0; a < 3; a++)
             for (int b = 0; b < 3; b++) {
-                const float w = float(wx[a] * wy[b]);
-                const int X = cx + a - 1, Y = cy + b - 1;
                 float add[kFrameChannels];
 #pragma unroll
-                for (int c = 0; c < kFrameChannels; c++) add[c] = w * vals[c];
-                add[1] = w * mp;
-                add[2] = w * mp * float(v.x);
-                add[3] = w * mp * float(v.y);
-                if (on) {
-                    const int li = (X - x0) * th + (Y - y0);
+                for (int c = 0; c < kFrameChannels; c++) add[c] = 0.0f;
 #pragma unroll
-                    for (int c = 0; c < kFrameChannels; c++) atomicAdd(&tile[c][li], add[c]);
-                } else {
-                    const size_t node = (size_t)X * gy + Y;
+                for (int j = 0; j < 4; j++) {
+                    const float wgt = wx[j][a] * wy[j][b];
 #pragma unroll
-                    for (int c = 0; c < kFrameChannels; c++) atomicAdd(&F.ch[c][node], add[c]);
+                    for (int c = 0; c < kFrameChannels; c++) add[c] += wgt * vals[j][c];
                 }
+                frame_node_add(tile, on, x0, y0, th, F, gy, cx + a - 1, cy + b - 1, add);
             }
-        atomicAdd(&F.count[(size_t)cx * gy + cy], 1u);
+        atomicAdd(&F.count[(size_t)cx * gy + cy], (uint32_t)nact);
+    } else if (nact > 0) {
+#pragma unroll 1
+        for (int j = 0; j < 4; j++) {
+            if (!act[j]) continue;
+            float vals[kFrameChannels], x, y, wx[3], wy[3];
+            frame_values(P, e0 + 32 * j, particle_mass, colors, ncolors, vals, x, y);
+            bspline(x, wx);
+            bspline(y, wy);
+            for (int a = 0; a < 3; a++)
+                for (int b = 0; b < 3; b++) {
+                    const float wgt = wx[a] * wy[b];
+                    float add[kFrameChannels];
+#pragma unroll
+                    for (int c = 0; c < kFrameChannels; c++) add[c] = wgt * vals[c];
+                    frame_node_add(tile, on, x0, y0, th, F, gy, cxs[j] + a - 1, cys[j] + b - 1, add);
+                }
+            atomicAdd(&F.count[(size_t)cxs[j] * gy + cys[j]], 1u);
+        }
     }
     __syncthreads();
     for (int k = threadIdx.x; k < nt; k += 256) {

@@ -149,7 +149,7 @@ __global__ void __launch_bounds__(256) k_frame_scatter(Pts<Real> P, int n, int g
         }
         int cx = 0, cy = 0;
 #pragma unroll
-        for (int j = 0; j < 4; j++) if (j == first || (first < 0 && j == 0)) { cx = cxs[j]; cy = cys[j]; }
+        for (int j = 0; j < 4; j++) if (j == first) { cx = cxs[j]; cy = cys[j]; }
         for (int a = 0; a < 3; a++)
             for (int b = 0; b < 3; b++) {
                 float add[kFrameChannels];

@@ -922,6 +922,7 @@ __device__ __forceinline__ void fused_chunk(ChunkSmem<Real, Acc, BT, PPT, CAP, S
                 Real sax = 0, say = 0, tax = 0, tay = 0;
 #pragma unroll
                 for (int b = 0; b < 3; b++) {
+                    if (a == 1 && b == 1) continue;   // the centre node's difference is zero
                     const Real dx = nv[a][b].x - ccx, dy = nv[a][b].y - ccy;
                     sax += wy[b] * dx; say += wy[b] * dy;
                     tax += gyv[b] * dx; tay += gyv[b] * dy;
@@ -936,9 +937,12 @@ __device__ __forceinline__ void fused_chunk(ChunkSmem<Real, Acc, BT, PPT, CAP, S
         }
         x += vx * kp.dt_h_inv;
         y += vy * kp.dt_h_inv;
-        if (isnan(vx + vy)) err |= kErrVelNan;
-        if (isnan(x + y)) err |= kErrPosNan;
-        if (isnan((c00 + c10) + (c01 + c11))) err |= kErrBpNan;
+        // one test in the usual case; a NaN in any of the sums reaches the total
+        if (isnan(((vx + vy) + (x + y)) + ((c00 + c10) + (c01 + c11)))) {
+            if (isnan(vx + vy)) err |= kErrVelNan;
+            if (isnan(x + y)) err |= kErrPosNan;
+            if (isnan((c00 + c10) + (c01 + c11))) err |= kErrBpNan;
+        }
         bool moved = false;
         if (x > Real(0.5)) { x -= Real(1); cx++; moved = true; }
         else if (x < Real(-0.5)) { x += Real(1); cx--; moved = true; }

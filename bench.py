@@ -23,8 +23,8 @@ partition, FP64, its own launch shapes) on the same scene, timed with CUDA
 events around its sub-step loop ("reference_gpu").
 
 --impl reference: the reference's own kernels (simulation/kernels.cuh,
-compiled for the host in oracle/_ref) advance a bounded sample of the same
-scene family on the host cores; rank 0 only.
+compiled for the host in oracle/_ref) advance the same scene on the host
+cores, P2G's blocks in parallel with atomic adds; rank 0 only.
 """
 import argparse
 import json
@@ -138,10 +138,8 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows), "power_w_max": max(pw) if pw else None}
 
 
-def make_scene(seed, max_points=None, sample=False, grid=None):
+def make_scene(seed, max_points=None, grid=None):
     from icempm_2d_sp_b200 import scenes
-    if sample:  # the same generation rules on a 1024x512 sub-domain (1/16 of the cells)
-        return scenes.floe_field(seed=seed, gx=1024, gy=512, n_seeds=125)
     if grid is not None:
         gx, gy = grid
         return scenes.floe_field(seed=seed, gx=gx, gy=gy, n_seeds=max(1, round(2000 * gx * gy / (4096 * 2048))))
@@ -149,24 +147,26 @@ def make_scene(seed, max_points=None, sample=False, grid=None):
 
 
 def run_reference(args, rank):
-    """The reference kernels on the host cores, one sub-step of the sample
-    scene per step."""
+    """The reference's own step on the host cores: simulation/kernels.cuh
+    compiled for the host (oracle/_ref), on the same scene as our arm, one
+    sub-step of the whole scene per step, P2G's blocks over all host threads
+    with atomic adds as on the GPU."""
     if rank != 0:
         return
-    sc = make_scene(1235, sample=True)
+    sc = make_scene(1235, max_points=args.max_points, grid=args.grid)
     grid = np.zeros((9, sc.grid_nodes))
     grid[5], grid[6] = sc.current[:sc.grid_nodes], sc.current[sc.grid_nodes:]
-    sample = (f"floe-field generation rules on a 1024x512 sub-domain (125 seeds), N={sc.n} points, "
-              f"one sub-step per step")
+    sample = f"the benchmark scene itself (N={sc.n} points, {sc.grid_nodes} nodes), one sub-step per step"
     try:
         from oracle.refbuild import build_ref
         L = build_ref.load()
         cores = int(L.ref_num_threads())
         kind = "reference"
-        run = lambda k, first: build_ref.run_steps(sc.prms, sc.soa, sc.n, grid, sc.status, k, first)
-        note = ("reference simulation/kernels.cuh compiled for the host (oracle/_ref); P2G serial "
-                "(its atomics emulated in order), grid update and G2P over OpenMP threads; "
-                "compat forcing (the reference has no wind term)")
+        run = lambda k, first: build_ref.run_steps(sc.prms, sc.soa, sc.n, grid, sc.status, k, first,
+                                                   parallel_p2g=True)
+        note = ("reference simulation/kernels.cuh compiled for the host (oracle/_ref); P2G, grid update and "
+                "G2P blocks over OpenMP threads, P2G's atomicAdd as relaxed atomic adds; compat forcing "
+                "(the reference has no wind term)")
     except (FileNotFoundError, OSError):
         import oracle
         cores = oracle.num_threads()
@@ -178,10 +178,12 @@ def run_reference(args, rank):
     run(args.steps, args.warmup)
     dt = time.perf_counter() - t0
     v = sc.n * args.steps / dt
+    workload = WORKLOAD if args.grid is None else WORKLOAD.replace("4096x2048", "%dx%d" % tuple(args.grid))
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": {"workload": WORKLOAD, "points": int(sc.n), "grid_nodes": sc.grid_nodes},
+            "data": "synthetic (seeded Voronoi floe-field generator)",
+            "config": {"workload": workload, "points": int(sc.n), "grid_nodes": sc.grid_nodes, "same_config": True},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample, "note": note},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)

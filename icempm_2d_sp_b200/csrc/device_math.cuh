@@ -39,6 +39,55 @@ template <class T> __device__ __forceinline__ void bspline(T x, T w[3])
     w[2] = T(0.5) * v2 * v2;
 }
 
+// ---- pairs -----------------------------------------------------------------
+// Two values that take the same arithmetic (the x and y components of a
+// velocity, a momentum or a matrix column) travel as one pair.  For float the
+// pair operations are sm_100's packed FP32x2 instructions (one instruction,
+// two lanes, each rounded exactly as the scalar operation); for double they
+// are two scalar operations.
+template <class T> struct PairOf;
+template <> struct PairOf<float> { using type = float2; };
+template <> struct PairOf<double> { using type = double2; };
+template <class T> using P2 = typename PairOf<T>::type;
+
+__device__ __forceinline__ float2 pbc(float s) { return make_float2(s, s); }
+__device__ __forceinline__ double2 pbc(double s) { return make_double2(s, s); }
+__device__ __forceinline__ float2 pmk(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ double2 pmk(double a, double b) { return make_double2(a, b); }
+
+__device__ __forceinline__ float2 padd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 pmul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 pfma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 psub(float2 a, float2 b)
+{
+    float2 r;
+    asm("{\n\t.reg .b64 pa, pb, pr;\n\t"
+        "mov.b64 pa, {%2, %3};\n\tmov.b64 pb, {%4, %5};\n\t"
+        "sub.rn.f32x2 pr, pa, pb;\n\tmov.b64 {%0, %1}, pr;\n}"
+        : "=f"(r.x), "=f"(r.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return r;
+}
+__device__ __forceinline__ double2 padd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 psub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 pmul(double2 a, double2 b) { return make_double2(a.x * b.x, a.y * b.y); }
+__device__ __forceinline__ double2 pfma(double2 a, double2 b, double2 c)
+{
+    return make_double2(fma(a.x, b.x, c.x), fma(a.y, b.y, c.y));
+}
+
+// B-spline weights of both components of a pair: w[k] = (w_k(v.x), w_k(v.y)).
+// With v = (x, x) every w[k] is a broadcast pair.  w[1] = 0.75 - x^2 is
+// formed as (0.5 - x)(x + 0.5) + 0.5.
+template <class PT> __device__ __forceinline__ void bspline2(PT v, PT w[3])
+{
+    using T = decltype(v.x);
+    const PT half = pbc(T(0.5));
+    const PT v0 = psub(half, v), v2 = padd(v, half);
+    w[0] = pmul(pmul(half, v0), v0);
+    w[1] = pfma(v0, v2, half);
+    w[2] = pmul(pmul(half, v2), v2);
+}
+
 // Kinematic invariants of F = I + H.
 //   Jm1 = det(F) - 1 = tr H + det H
 //   dev(b) = [[d, b01], [b01, -d]] with b = F F^T  (b - I = H + H^T + H H^T)

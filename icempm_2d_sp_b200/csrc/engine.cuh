@@ -65,6 +65,11 @@
 #ifndef ICEMPM_FUSED_STAGES
 #define ICEMPM_FUSED_STAGES 1
 #endif
+// 1: the fused kernel keeps the 3x3 node velocities of the last cell in
+// registers for the thread's next point; 0: it loads them for every point.
+#ifndef ICEMPM_VEL_CACHE
+#define ICEMPM_VEL_CACHE 0
+#endif
 // 1: persistent grid of as many CTAs as fit; 0: one CTA per chunk.
 #ifndef ICEMPM_FUSED_PERSIST
 #define ICEMPM_FUSED_PERSIST 1
@@ -317,7 +322,7 @@ __device__ __forceinline__ void src_terms(const Src<Real> &s, int a, int b, Real
 // The tile covers nodes [x0, x0+tw) x [y0, y0+th) of the grid; entry
 // (X - x0) * th + (Y - y0), three channels.
 template <class Acc, int CAP> struct Tile {
-    Acc (*t)[CAP];
+    Acc (*t)[CAP > 0 ? CAP : 1];
     int x0, y0, tw, th;
     unsigned th_rcp;   // ceil(2^32 / th): entry k lies in column umulhi(k, th_rcp) (exact while k * th < 2^32)
     bool on;
@@ -592,14 +597,23 @@ __device__ __forceinline__ bool mbar_wait_bounded(unsigned long long *bar, uint3
 }
 
 // A thread accumulates its points' node terms in a register patch of the
-// 3x3 nodes around cell (cx, cy).  When the next point sits one cell higher
-// in the same column the patch slides: its lowest node row is written out and
-// the other two rows move down.  Any other cell change writes out the patch.
+// 3x3 nodes around cell (cx, cy): mass m[a][b] and momentum p[a][b] = (px, py).
+// When the next point sits one cell higher in the same column the patch
+// slides: its lowest node row is written out and the other two rows move
+// down.  Any other cell change writes out the patch.
 template <class Real> struct Patch {
-    Real m[3][3], px[3][3], py[3][3];
+    Real m[3][3];
+    P2<Real> p[3][3];
     int cx, cy;
     bool have, in_tile;
 };
+
+template <class Real, class Acc, int CAP>
+__device__ __forceinline__ void patch_node(const Patch<Real> &p, const Tile<Acc, CAP> &T, const AccGrid<Acc> &gacc,
+                                           int gy, int a, int b)
+{
+    node_add<Real, Acc, CAP>(T, p.in_tile, gacc, gy, p.cx + a - 1, p.cy + b - 1, p.m[a][b], p.p[a][b].x, p.p[a][b].y);
+}
 
 template <class Real, class Acc, int CAP>
 __device__ __forceinline__ void patch_flush(Patch<Real> &p, const Tile<Acc, CAP> &T, const AccGrid<Acc> &gacc, int gy)
@@ -607,23 +621,7 @@ __device__ __forceinline__ void patch_flush(Patch<Real> &p, const Tile<Acc, CAP>
 #pragma unroll
     for (int a = 0; a < 3; a++)
 #pragma unroll
-        for (int b = 0; b < 3; b++)
-            node_add<Real, Acc, CAP>(T, p.in_tile, gacc, gy, p.cx + a - 1, p.cy + b - 1, p.m[a][b], p.px[a][b], p.py[a][b]);
-    p.have = false;
-}
-
-// Writes out a tile patch with its lowest (b = 0) and highest (b = 2) node
-// rows only where asked: a row another lane has taken over is skipped.
-template <class Real, class Acc, int CAP>
-__device__ __forceinline__ void patch_flush_rows(Patch<Real> &p, const Tile<Acc, CAP> &T, const AccGrid<Acc> &gacc, int gy,
-                                                 bool low, bool high)
-{
-#pragma unroll
-    for (int a = 0; a < 3; a++) {
-        if (low) node_add<Real, Acc, CAP>(T, p.in_tile, gacc, gy, p.cx + a - 1, p.cy - 1, p.m[a][0], p.px[a][0], p.py[a][0]);
-        node_add<Real, Acc, CAP>(T, p.in_tile, gacc, gy, p.cx + a - 1, p.cy, p.m[a][1], p.px[a][1], p.py[a][1]);
-        if (high) node_add<Real, Acc, CAP>(T, p.in_tile, gacc, gy, p.cx + a - 1, p.cy + 1, p.m[a][2], p.px[a][2], p.py[a][2]);
-    }
+        for (int b = 0; b < 3; b++) patch_node<Real, Acc, CAP>(p, T, gacc, gy, a, b);
     p.have = false;
 }
 
@@ -637,10 +635,10 @@ __device__ __forceinline__ void patch_flush_rows(Patch<Real> &p, const Tile<Acc,
 // it).  In the usual case 9 of the 27 node-channel adds remain.  All 32
 // lanes of the warp must call it.
 template <class Real>
-__device__ __forceinline__ void patch_merge(Patch<Real> &p, int lane, bool &low, bool &high)
+__device__ __forceinline__ void patch_merge(Patch<Real> &p, int lane, bool &low, bool &high, bool tile_only = true)
 {
     const unsigned FULL = 0xffffffffu;
-    const bool mine = p.have && p.in_tile;
+    const bool mine = p.have && (p.in_tile || !tile_only);
     const uint32_t key = mine ? (((uint32_t)p.cx << 16) | (uint32_t)p.cy) : 0xffffffffu;
     const uint32_t key_up = __shfl_down_sync(FULL, key, 1);     // lane l+1
     const uint32_t key_dn = __shfl_up_sync(FULL, key, 1);       // lane l-1
@@ -648,12 +646,12 @@ __device__ __forceinline__ void patch_merge(Patch<Real> &p, int lane, bool &low,
     const bool below = mine && lane > 0 && key_dn == key - 1u;
 #pragma unroll
     for (int a = 0; a < 3; a++) {
-        const Real um = __shfl_down_sync(FULL, p.m[a][0], 1), ux = __shfl_down_sync(FULL, p.px[a][0], 1),
-                   uy = __shfl_down_sync(FULL, p.py[a][0], 1);
-        const Real dm = __shfl_up_sync(FULL, p.m[a][2], 1), dx = __shfl_up_sync(FULL, p.px[a][2], 1),
-                   dy = __shfl_up_sync(FULL, p.py[a][2], 1);
-        if (above) { p.m[a][1] += um; p.px[a][1] += ux; p.py[a][1] += uy; }
-        if (below) { p.m[a][1] += dm; p.px[a][1] += dx; p.py[a][1] += dy; }
+        const Real um = __shfl_down_sync(FULL, p.m[a][0], 1), ux = __shfl_down_sync(FULL, p.p[a][0].x, 1),
+                   uy = __shfl_down_sync(FULL, p.p[a][0].y, 1);
+        const Real dm = __shfl_up_sync(FULL, p.m[a][2], 1), dx = __shfl_up_sync(FULL, p.p[a][2].x, 1),
+                   dy = __shfl_up_sync(FULL, p.p[a][2].y, 1);
+        if (above) { p.m[a][1] += um; p.p[a][1].x += ux; p.p[a][1].y += uy; }
+        if (below) { p.m[a][1] += dm; p.p[a][1].x += dx; p.p[a][1].y += dy; }
     }
     low = !below;
     high = !above;
@@ -676,8 +674,8 @@ __device__ __forceinline__ void patch_store(const Patch<Real> &p, const Tile<Acc
         for (int b = 0; b < 3; b++) {
             if (on && (b != 0 || low) && (b != 2 || high)) {
                 const int li = base + a * T.th + b;
-                const Acc am = AccOps<Acc>::cvt(p.m[a][b]), ax = AccOps<Acc>::cvt(p.px[a][b]),
-                          ay = AccOps<Acc>::cvt(p.py[a][b]);
+                const Acc am = AccOps<Acc>::cvt(p.m[a][b]), ax = AccOps<Acc>::cvt(p.p[a][b].x),
+                          ay = AccOps<Acc>::cvt(p.p[a][b].y);
                 if (ATOMIC) {
                     AccOps<Acc>::add_shared(&T.t[0][li], am);
                     AccOps<Acc>::add_shared(&T.t[1][li], ax);
@@ -693,33 +691,39 @@ __device__ __forceinline__ void patch_store(const Patch<Real> &p, const Tile<Acc
         }
 }
 
-// The node terms of src_terms, summed separably: with
-//   u_a = m wx_a,  p_a = wx_a (ax + s00 (a-1)),  q_a = wx_a s01,
-//   r_a = wx_a (ay + s10 (a-1)),  t_a = wx_a s11,
-// node (a, b) receives  m: u_a wy_b,  px: wy_b (p_a + (b-1) q_a),  py: wy_b (r_a + (b-1) t_a).
-template <class Real> __device__ __forceinline__ void patch_accumulate(Patch<Real> &p, const Src<Real> &s)
+// P2G source of one point in pair form (scaled for fixed point): node (a, b)
+// receives  m: mp wx_a wy_b  and  (px, py): wx_a wy_b (A + (a-1) S0 + (b-1) S1)
+// with A = (ax, ay), S0 = h (S00, S10), S1 = h (S01, S11) (see make_src).
+template <class Real> struct SrcP {
+    int cx, cy;
+    Real x, y, mp;
+    P2<Real> A, S0, S1;
+};
+
+// The node terms, summed separably over the weights of both axes.
+template <class Real> __device__ __forceinline__ void patch_accumulate(Patch<Real> &p, const SrcP<Real> &s)
 {
-    const Real axa[3] = {s.ax - s.s00, s.ax, s.ax + s.s00};
-    const Real aya[3] = {s.ay - s.s10, s.ay, s.ay + s.s10};
+    using PT = P2<Real>;
+    PT wx[3], wy[3];
+    bspline2(pbc(s.x), wx);
+    bspline2(pbc(s.y), wy);
+    const PT axa[3] = {psub(s.A, s.S0), s.A, padd(s.A, s.S0)};
 #pragma unroll
     for (int a = 0; a < 3; a++) {
-        const Real u = s.mp * s.wx[a];
-        const Real pa = s.wx[a] * axa[a], qa = s.wx[a] * s.s01;
-        const Real ra = s.wx[a] * aya[a], ta = s.wx[a] * s.s11;
-        p.m[a][0] += u * s.wy[0];
-        p.m[a][1] += u * s.wy[1];
-        p.m[a][2] += u * s.wy[2];
-        p.px[a][0] += s.wy[0] * (pa - qa);
-        p.px[a][1] += s.wy[1] * pa;
-        p.px[a][2] += s.wy[2] * (pa + qa);
-        p.py[a][0] += s.wy[0] * (ra - ta);
-        p.py[a][1] += s.wy[1] * ra;
-        p.py[a][2] += s.wy[2] * (ra + ta);
+        const PT pr = pmul(wx[a], axa[a]);
+        const PT qt = pmul(wx[a], s.S1);
+        p.p[a][0] = pfma(wy[0], psub(pr, qt), p.p[a][0]);
+        p.p[a][1] = pfma(wy[1], pr, p.p[a][1]);
+        p.p[a][2] = pfma(wy[2], padd(pr, qt), p.p[a][2]);
+        const Real u = s.mp * wx[a].x;
+        p.m[a][0] = fma(u, wy[0].x, p.m[a][0]);
+        p.m[a][1] = fma(u, wy[1].x, p.m[a][1]);
+        p.m[a][2] = fma(u, wy[2].x, p.m[a][2]);
     }
 }
 
 template <class Real, class Acc, int CAP>
-__device__ __forceinline__ void patch_add(Patch<Real> &p, const Src<Real> &s, const Tile<Acc, CAP> &T,
+__device__ __forceinline__ void patch_add(Patch<Real> &p, const SrcP<Real> &s, const Tile<Acc, CAP> &T,
                                           const AccGrid<Acc> &gacc, int gy)
 {
     if (p.have) {
@@ -728,10 +732,10 @@ __device__ __forceinline__ void patch_add(Patch<Real> &p, const Src<Real> &s, co
         if (slide) {
 #pragma unroll
             for (int a = 0; a < 3; a++) {
-                node_add<Real, Acc, CAP>(T, p.in_tile, gacc, gy, p.cx + a - 1, p.cy - 1, p.m[a][0], p.px[a][0], p.py[a][0]);
-                p.m[a][0] = p.m[a][1]; p.px[a][0] = p.px[a][1]; p.py[a][0] = p.py[a][1];
-                p.m[a][1] = p.m[a][2]; p.px[a][1] = p.px[a][2]; p.py[a][1] = p.py[a][2];
-                p.m[a][2] = Real(0); p.px[a][2] = Real(0); p.py[a][2] = Real(0);
+                patch_node<Real, Acc, CAP>(p, T, gacc, gy, a, 0);
+                p.m[a][0] = p.m[a][1]; p.p[a][0] = p.p[a][1];
+                p.m[a][1] = p.m[a][2]; p.p[a][1] = p.p[a][2];
+                p.m[a][2] = Real(0); p.p[a][2] = pbc(Real(0));
             }
             p.cy += 1;
         } else if (!same) {
@@ -742,7 +746,7 @@ __device__ __forceinline__ void patch_add(Patch<Real> &p, const Src<Real> &s, co
 #pragma unroll
         for (int a = 0; a < 3; a++)
 #pragma unroll
-            for (int b = 0; b < 3; b++) { p.m[a][b] = Real(0); p.px[a][b] = Real(0); p.py[a][b] = Real(0); }
+            for (int b = 0; b < 3; b++) { p.m[a][b] = Real(0); p.p[a][b] = pbc(Real(0)); }
         p.cx = s.cx; p.cy = s.cy;
         p.in_tile = cell_in_tile(T, s.cx, s.cy);
         p.have = true;
@@ -753,20 +757,49 @@ __device__ __forceinline__ void patch_add(Patch<Real> &p, const Src<Real> &s, co
 // Shared memory of one CTA of the fused kernel.  A chunk is CH = BT*PPT
 // consecutive points; the stages hold the point state of the current chunk
 // (and with two stages the next one), which the bulk copy engine fetches
-// ahead; `tile` holds the scatter accumulators of the chunk's cells +-2 nodes.
+// ahead; `tile` holds the scatter accumulators of the chunk's new cells +-1
+// node.  After a point's G2P the stage entries of that point hold its P2G
+// source (see fused_chunk); `mp` carries the source's mass where the K entry
+// has no room for it (FP64 state).
 template <class Real, class Acc, int BT, int PPT, int CAP, int STAGES> struct ChunkSmem {
     static constexpr int CH = BT * PPT;
     struct Stage {
         V4<Real> A[CH];
         V4<Real> H[CH];
         uint2 K[CH];
+        Real mp[sizeof(Real) == 8 ? CH : 1];
     };
     Stage stage[STAGES];
-    Acc tile[3][CAP];
+    Acc tile[3][CAP > 0 ? CAP : 1];
     unsigned long long mbar[2];
     int red[BT / 32][5];
     int wbox[BT / 32][5];   // per warp: node box of its end patches {x0, x1, y0, y1}, duplicate cells
 };
+
+// Cell word of a stage entry whose point scatters nothing this step.
+constexpr uint32_t kNoScatter = 0xffffffffu;
+
+// The source's mass: in the K entry's second word (FP32 state, returned as
+// that word) or in the stage's mass array (FP64 state, returns 0).
+template <class Stage> __device__ __forceinline__ uint32_t put_src_mass(Stage &, int, float mp)
+{
+    return __float_as_uint(mp);
+}
+template <class Stage> __device__ __forceinline__ uint32_t put_src_mass(Stage &sg, int local, double mp)
+{
+    sg.mp[local] = mp;
+    return 0u;
+}
+template <class Real, class Stage> __device__ __forceinline__ Real get_src_mass(const Stage &sg, int local, uint2 k)
+{
+    if constexpr (sizeof(Real) == 4) return __uint_as_float(k.y);
+    else return sg.mp[local];
+}
+
+template <class Real> __device__ __forceinline__ P2<Real> ld_vel(const V2<Real> *p)
+{
+    return *reinterpret_cast<const P2<Real> *>(p);
+}
 
 template <class Real, class Stage>
 __device__ __forceinline__ void fetch_chunk(Stage &sg, const Pts<Real> &P, uint32_t base, int ch,
@@ -780,24 +813,10 @@ __device__ __forceinline__ void fetch_chunk(Stage &sg, const Pts<Real> &P, uint3
     bulk_to_smem(sg.K, P.K + base, bk, bar);
 }
 
-// G2P follows partition_kernel_g2p (kernels.cuh:181-315).  The 3x3 gather is
-// evaluated separably: with s_a = sum_b wy_b (v_ab - v_c) and
-// t_a = sum_b wy_b (b-1-y) (v_ab - v_c), v_c the centre node,
-//   v_p = v_c + sum_a wx_a s_a
-//   C[:,0] = 4/h sum_a wx_a (a-1-x) s_a,   C[:,1] = 4/h sum_a wx_a t_a,
-// which equals the reference's sums over the nine nodes (the subtracted v_c
-// cancels because sum_a wx_a (a-1-x) = 0 and sum_b wy_b (b-1-y) = 0) and keeps
-// FP32 roundoff relative to velocity differences.
-//
-// Persistent CTAs walk the chunks c = blockIdx.x, blockIdx.x + gridDim.x, ...
-// The point state of a chunk (A, H, K: 40 B per point in FP32) arrives in
-// shared memory by bulk copy, issued ahead of its use; the G2P gathers read
-// grid velocities through L1; new point state is written to global memory
-// with streaming stores; the P2G terms go through register patches into the
-// shared tile and from there, one atomic per node and channel, to the global
-// accumulators.  Every point of a chunk is read and written by the same
-// thread, so a stage can be refilled as soon as the CTA has passed the
-// barrier after its points.
+// Orders this thread's generic-proxy writes to shared memory before later
+// bulk copies (async proxy) into the same bytes.
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
 // Records one projection onto the yield surface (case 3 of wolper_dp) for the
 // learned return map: the trial singular values (sv), Jp_inv before (jp0) and
 // after, and the singular values of the projected state (H).
@@ -823,6 +842,30 @@ __device__ __noinline__ void harvest_record(HarvestBuf *hb, const MatT<Real> &m,
 // are read.  Error bits and the count of newly disabled points accumulate
 // into err, perr, ndis.  HARVEST: the instance that records return-map pairs
 // (kept out of the ordinary instance, whose registers it would crowd).
+//
+// G2P follows partition_kernel_g2p (kernels.cuh:181-315), P2G
+// partition_kernel_p2g (kernels.cuh:39-104).  Two phases per chunk:
+//  1. per point: the 3x3 gather, advection and re-keying, the Fe update and
+//     the return map, the stores of the new state, and the P2G source of the
+//     new state, written back into the point's own stage entries (A <- x, y,
+//     S1; H <- A, S0; K <- cell, mass).  The 3x3 node velocities (and the
+//     forcing entry) are loaded once per cell: after the locality sort a
+//     thread's points mostly share one cell.
+//  2. per point: the source's node terms into the thread's register patch;
+//     then the patches go through the shared tile (the chunk's new cells +-1
+//     node) to the global accumulators.
+// Splitting the chunk keeps the velocity cache and the patch from being live
+// at the same time.  Every point of a chunk is read and written by the same
+// thread, so the stage entries need no barrier between the phases.
+//
+// The gather is evaluated separably: with d_ab = v_ab - v_c (v_c the centre
+// node), S_a = sum_b wy_b d_ab and T_a = sum_b wy_b (b-1-y) d_ab,
+//   v_p = v_c + sum_a wx_a S_a,
+//   C[:,0] = 4/h sum_a wx_a (a-1-x) S_a,   C[:,1] = 4/h sum_a wx_a T_a,
+// which equals the reference's sums over the nine nodes (the subtracted v_c
+// cancels because sum_a wx_a (a-1-x) = 0 and sum_b wy_b (b-1-y) = 0) and keeps
+// FP32 roundoff relative to velocity differences.  Velocities, momenta and
+// the columns of C are pairs (packed FP32x2 arithmetic).
 template <class Real, class Acc, int BT, int PPT, int CAP, int STAGES, bool HARVEST>
 __device__ __forceinline__ void fused_chunk(ChunkSmem<Real, Acc, BT, PPT, CAP, STAGES> &sm, int s,
                                             const KParams<Real> &kp, const Pts<Real> &P, const Grid<Real, Acc> &G,
@@ -831,59 +874,21 @@ __device__ __forceinline__ void fused_chunk(ChunkSmem<Real, Acc, BT, PPT, CAP, S
                                             int &ndis)
 {
     using SM = ChunkSmem<Real, Acc, BT, PPT, CAP, STAGES>;
+    using PT = P2<Real>;
     constexpr int CH = SM::CH;
     constexpr int NW = BT / 32;
+    constexpr bool FIXED = AccOps<Acc>::fixed;
+    constexpr bool TILE = CAP > 0;
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-    const typename SM::Stage &sg = sm.stage[s];
+    typename SM::Stage &sg = sm.stage[s];
     const int wbase = wid * 32 * PPT + lane;
 
-    // box of the chunk's enabled, in-range cells
-    unsigned xmn = 0xffffu, ymn = 0xffffu, xmx = 0, ymx = 0;
+    // ---- phase 1 ----------------------------------------------------------
+    unsigned xmn = 0xffffu, ymn = 0xffffu, xmx = 0, ymx = 0;   // box of the new cells that scatter
     bool any = false;
-#pragma unroll
-    for (int j = 0; j < PPT; j++) {
-        const int local = wbase + 32 * j;
-        if (base + (uint32_t)local < (uint32_t)n) {
-            const uint2 key = sg.K[local];
-            const int cx = (int)(key.x & 0xffff), cy = (int)(key.x >> 16);
-            if (!(key.y & kDisabled) && cell_in_range(cx, cy, kp.gx, kp.gy)) {
-                xmn = min(xmn, (unsigned)cx); ymn = min(ymn, (unsigned)cy);
-                xmx = max(xmx, (unsigned)cx); ymx = max(ymx, (unsigned)cy);
-                any = true;
-            }
-        }
-    }
-    {
-        const unsigned FULL = 0xffffffffu;
-        xmn = __reduce_min_sync(FULL, xmn); ymn = __reduce_min_sync(FULL, ymn);
-        xmx = __reduce_max_sync(FULL, xmx); ymx = __reduce_max_sync(FULL, ymx);
-        const unsigned wany = __reduce_or_sync(FULL, any ? 1u : 0u);
-        if (lane == 0) {
-            sm.red[wid][0] = (int)xmn; sm.red[wid][1] = (int)ymn;
-            sm.red[wid][2] = (int)xmx; sm.red[wid][3] = (int)ymx; sm.red[wid][4] = (int)wany;
-        }
-    }
-    __syncthreads();
-    int bx0 = 0xffff, by0 = 0xffff, bx1 = 0, by1 = 0, bany = 0;
-#pragma unroll
-    for (int w = 0; w < NW; w++) {
-        bx0 = min(bx0, sm.red[w][0]); by0 = min(by0, sm.red[w][1]);
-        bx1 = max(bx1, sm.red[w][2]); by1 = max(by1, sm.red[w][3]); bany |= sm.red[w][4];
-    }
-    // scatter tile: cells +-2 (a point moves at most one cell per step)
-    Tile<Acc, CAP> T;
-    T.t = sm.tile;
-    T.x0 = bx0 - 2; T.y0 = by0 - 2;
-    T.tw = bx1 - bx0 + 5; T.th = by1 - by0 + 5;
-    // 64-bit products: a box spanning the whole grid must not wrap into range
-    T.on = bany && (long long)T.tw * (long long)T.th <= (long long)CAP;
-    if (!T.on) { T.tw = 0; T.th = 0; }
-    T.th_rcp = rcp32(T.th);
-    tile_zero<Acc, CAP, BT>(T);
-    __syncthreads();
-
-    Patch<Real> patch;
-    patch.have = false; patch.in_tile = false; patch.cx = patch.cy = 0;
+    uint32_t vcell = kNoScatter;   // cell whose node velocities vc, dv and forcing fc are held
+    PT vc = pbc(Real(0)), dv[8];
+    V4<Real> fc{};
 #pragma unroll 1
     for (int j = 0; j < PPT; j++) {
         const int local = wbase + 32 * j;
@@ -891,58 +896,75 @@ __device__ __forceinline__ void fused_chunk(ChunkSmem<Real, Acc, BT, PPT, CAP, S
         if (i >= (uint32_t)n) break;
         const uint2 key = sg.K[local];
         uint32_t util = key.y;
-        if (util & kDisabled) continue;
+        if (util & kDisabled) { sg.K[local].x = kNoScatter; continue; }
         const V4<Real> A = sg.A[local];
         const V4<Real> Hv = sg.H[local];
-        Real x = A.x, y = A.y, Jp = A.z;
+        Real Jp = A.z;
         const Real thick = A.w;
         M2<Real> H = {Hv.x, Hv.y, Hv.z, Hv.w};
         int cx = (int)(key.x & 0xffff), cy = (int)(key.x >> 16);
-        // forcing entry of the current cell, loaded early (points rarely change cell)
-        V4<Real> frc{};
-        if (kp.ext && cell_in_range(cx, cy, kp.gx, kp.gy)) frc = G.frc[(uint32_t)cx * (uint32_t)kp.gy + (uint32_t)cy];
-        Real vx = 0, vy = 0, c00 = 0, c01 = 0, c10 = 0, c11 = 0;
+        PT v = pbc(Real(0)), c0 = pbc(Real(0)), c1 = pbc(Real(0));   // (vx, vy), (c00, c10), (c01, c11)
         if (cell_in_range(cx, cy, kp.gx, kp.gy)) {
-            Real wx[3], wy[3];
-            bspline(x, wx);
-            bspline(y, wy);
-            V2<Real> nv[3][3];
+            if (!ICEMPM_VEL_CACHE || key.x != vcell) {
+                vcell = key.x;
+                const V2<Real> *col = G.vel + ((uint32_t)(cx - 1) * (uint32_t)kp.gy + (uint32_t)(cy - 1));
+                PT nv[3][3];
 #pragma unroll
-            for (int a = 0; a < 3; a++) {
-                const uint32_t col = (uint32_t)(cx + a - 1) * (uint32_t)kp.gy + (uint32_t)(cy - 1);
+                for (int a = 0; a < 3; a++)
 #pragma unroll
-                for (int b = 0; b < 3; b++) nv[a][b] = G.vel[col + b];
+                    for (int b = 0; b < 3; b++) nv[a][b] = ld_vel(col + (uint32_t)a * (uint32_t)kp.gy + b);
+                vc = nv[1][1];
+                int k = 0;
+#pragma unroll
+                for (int a = 0; a < 3; a++)
+#pragma unroll
+                    for (int b = 0; b < 3; b++)
+                        if (a != 1 || b != 1) dv[k++] = psub(nv[a][b], vc);
+                if (kp.ext) fc = G.frc[(uint32_t)cx * (uint32_t)kp.gy + (uint32_t)cy];
             }
-            const Real gyv[3] = {wy[0] * (Real(-1) - y), wy[1] * (-y), wy[2] * (Real(1) - y)};
-            const Real gxv[3] = {wx[0] * (Real(-1) - x), wx[1] * (-x), wx[2] * (Real(1) - x)};
-            const Real ccx = nv[1][1].x, ccy = nv[1][1].y;
-            Real sx = 0, sy = 0, px = 0, py = 0, qx = 0, qy = 0;
-#pragma unroll
-            for (int a = 0; a < 3; a++) {
-                Real sax = 0, say = 0, tax = 0, tay = 0;
-#pragma unroll
-                for (int b = 0; b < 3; b++) {
-                    if (a == 1 && b == 1) continue;   // the centre node's difference is zero
-                    const Real dx = nv[a][b].x - ccx, dy = nv[a][b].y - ccy;
-                    sax += wy[b] * dx; say += wy[b] * dy;
-                    tax += gyv[b] * dx; tay += gyv[b] * dy;
-                }
-                sx += wx[a] * sax; sy += wx[a] * say;     // v_p - v_c
-                px += gxv[a] * sax; py += gxv[a] * say;   // x-derivative part
-                qx += wx[a] * tax; qy += wx[a] * tay;     // y-derivative part
+            // column sums first (weights of y), then the row combination (weights of x),
+            // so that only one axis's weight pairs are live at a time
+            const PT one = pbc(Real(1));
+            PT sa[3], ta[3];
+            {
+                PT wy[3];
+                bspline2(pbc(A.y), wy);
+                const PT ny = pbc(-A.y);
+                const PT gy[3] = {pmul(wy[0], psub(ny, one)), pmul(wy[1], ny), pmul(wy[2], padd(ny, one))};
+                // a = 0: dv[0..2] are nodes (0, 0..2); a = 1: dv[3], dv[4] are nodes (1, 0), (1, 2)
+                // (the centre's difference is zero); a = 2: dv[5..7] are nodes (2, 0..2)
+                sa[0] = pfma(wy[2], dv[2], pfma(wy[1], dv[1], pmul(wy[0], dv[0])));
+                ta[0] = pfma(gy[2], dv[2], pfma(gy[1], dv[1], pmul(gy[0], dv[0])));
+                sa[1] = pfma(wy[2], dv[4], pmul(wy[0], dv[3]));
+                ta[1] = pfma(gy[2], dv[4], pmul(gy[0], dv[3]));
+                sa[2] = pfma(wy[2], dv[7], pfma(wy[1], dv[6], pmul(wy[0], dv[5])));
+                ta[2] = pfma(gy[2], dv[7], pfma(gy[1], dv[6], pmul(gy[0], dv[5])));
             }
-            vx = ccx + sx; vy = ccy + sy;
-            c00 = kp.four_h_inv * px; c10 = kp.four_h_inv * py;
-            c01 = kp.four_h_inv * qx; c11 = kp.four_h_inv * qy;
+            PT sv, pv, qv;
+            {
+                PT wx[3];
+                bspline2(pbc(A.x), wx);
+                const PT nx = pbc(-A.x);
+                const PT gx[3] = {pmul(wx[0], psub(nx, one)), pmul(wx[1], nx), pmul(wx[2], padd(nx, one))};
+                sv = pfma(wx[2], sa[2], pfma(wx[1], sa[1], pmul(wx[0], sa[0])));
+                pv = pfma(gx[2], sa[2], pfma(gx[1], sa[1], pmul(gx[0], sa[0])));
+                qv = pfma(wx[2], ta[2], pfma(wx[1], ta[1], pmul(wx[0], ta[0])));
+            }
+            v = padd(vc, sv);
+            const PT fh = pbc(kp.four_h_inv);
+            c0 = pmul(fh, pv);
+            c1 = pmul(fh, qv);
         }
-        x += vx * kp.dt_h_inv;
-        y += vy * kp.dt_h_inv;
-        // one test in the usual case; a NaN in any of the sums reaches the total
-        if (isnan(((vx + vy) + (x + y)) + ((c00 + c10) + (c01 + c11)))) {
-            if (isnan(vx + vy)) err |= kErrVelNan;
-            if (isnan(x + y)) err |= kErrPosNan;
-            if (isnan((c00 + c10) + (c01 + c11))) err |= kErrBpNan;
+        const PT xy = pfma(v, pbc(kp.dt_h_inv), pmk(A.x, A.y));
+        {   // one test in the usual case; a NaN in any of the sums reaches the total
+            const PT t = padd(padd(v, xy), padd(c0, c1));
+            if (isnan(t.x + t.y)) {
+                if (isnan(v.x + v.y)) err |= kErrVelNan;
+                if (isnan(xy.x + xy.y)) err |= kErrPosNan;
+                if (isnan((c0.x + c0.y) + (c1.x + c1.y))) err |= kErrBpNan;
+            }
         }
+        Real x = xy.x, y = xy.y;
         bool moved = false;
         if (x > Real(0.5)) { x -= Real(1); cx++; moved = true; }
         else if (x < Real(-0.5)) { x += Real(1); cx--; moved = true; }
@@ -956,7 +978,7 @@ __device__ __forceinline__ void fused_chunk(ChunkSmem<Real, Acc, BT, PPT, CAP, S
 
         // Fe <- (I + dt C) Fe, i.e. H <- H + D + D H with D = dt C
         {
-            const Real d00 = kp.dt * c00, d01 = kp.dt * c01, d10 = kp.dt * c10, d11 = kp.dt * c11;
+            const Real d00 = kp.dt * c0.x, d01 = kp.dt * c1.x, d10 = kp.dt * c0.y, d11 = kp.dt * c1.y;
             const M2<Real> h = H;
             H.a00 = h.a00 + d00 + (d00 * h.a00 + d01 * h.a10);
             H.a01 = h.a01 + d01 + (d00 * h.a01 + d01 * h.a11);
@@ -969,11 +991,11 @@ __device__ __forceinline__ void fused_chunk(ChunkSmem<Real, Acc, BT, PPT, CAP, S
         pq(k, kp.mat.mu, kp.mat.kappa, p_tr, q_tr);
         if (!(util & kCrushed)) util = failure_check(kp.mat, util, p_tr, q_tr);
         if (util & kCrushed) {
-            const SvdH<Real> sv = svd_h(H);
+            const SvdH<Real> svd = svd_h(H);
             const Real jp0 = Jp;
-            wolper_dp(kp.mat, thick, p_tr, q_tr, k, sv, H, Jp);
+            wolper_dp(kp.mat, thick, p_tr, q_tr, k, svd, H, Jp);
             if (HARVEST && kp.harvest && (i + (uint32_t)step) % (uint32_t)kp.harvest_stride == 0u)
-                harvest_record(kp.harvest, kp.mat, sv, p_tr, q_tr, jp0, thick, H, Jp);
+                harvest_record(kp.harvest, kp.mat, svd, p_tr, q_tr, jp0, thick, H, Jp);
             if (isnan((H.a00 + H.a10) + (H.a01 + H.a11))) err |= kErrFeNan;
             k = kinematics(H);
         }
@@ -983,9 +1005,9 @@ __device__ __forceinline__ void fused_chunk(ChunkSmem<Real, Acc, BT, PPT, CAP, S
         V4<Real> Ho; Ho.x = H.a00; Ho.y = H.a01; Ho.z = H.a10; Ho.w = H.a11;
         st_stream(P.H + i, Ho);
         if (store_vc || (util & kDisabled)) {   // a point disabled now keeps this step's V and C
-            V2<Real> Vo; Vo.x = vx; Vo.y = vy;
+            V2<Real> Vo; Vo.x = v.x; Vo.y = v.y;
             st_stream(P.V + i, Vo);
-            V4<Real> Co; Co.x = c00; Co.y = c01; Co.z = c10; Co.w = c11;
+            V4<Real> Co; Co.x = c0.x; Co.y = c1.x; Co.z = c0.y; Co.w = c1.y;
             st_stream(P.C + i, Co);
         }
         const uint32_t cell = ((uint32_t)cy << 16) | (uint32_t)cx;   // as kernels.cuh:305
@@ -995,28 +1017,137 @@ __device__ __forceinline__ void fused_chunk(ChunkSmem<Real, Acc, BT, PPT, CAP, S
         }
         if (recordPQ) { V2<Real> pqv; pqv.x = p_tr; pqv.y = q_tr; st_stream(P.PQ + i, pqv); }
 
+        // P2G source of the new state (make_src in pair form): with
+        // S = m_p C - dt_vol_Dpinv Jp_inv thickness tau (columns S0, S1),
+        // A = m_p v - h (S0 x + S1 y) (+ the extended forcing's impulse).
+        uint2 src_key = make_uint2(kNoScatter, 0u);   // new cell and mass of the source, or no scatter
         if (!(util & kDisabled)) {
             if (cell_in_range(cx, cy, kp.gx, kp.gy)) {
-                Src<Real> src;
-                src.cx = cx; src.cy = cy;
-                if (kp.ext && moved) frc = G.frc[(uint32_t)cx * (uint32_t)kp.gy + (uint32_t)cy];
-                make_src<Real, Acc>(kp, frc, src, x, y, Jp, thick, k, vx, vy, c00, c01, c10, c11, perr);
-                // NaN reaches these sums from any NaN term (the scatter's NaN checks)
-                const Real sw = (src.wx[0] + src.wx[1] + src.wx[2]) + (src.wy[0] + src.wy[1] + src.wy[2]);
-                if (isnan(sw + src.mp)) perr |= kErrP2gNanMass;
-                if (isnan(sw + ((src.ax + src.ay) + (src.s00 + src.s01) + (src.s10 + src.s11)))) perr |= kErrP2gNanVel;
-                patch_add<Real, Acc, CAP>(patch, src, T, G.acc, kp.gy);
+                const M2<Real> tau = kirchhoff(k, kp.mat.mu, kp.mat.kappa);
+                const Real mp = kp.particle_mass * thick;
+                const PT nsc = pbc(-(kp.dt_vol_Dpinv * Jp * thick)), mpp = pbc(mp);
+                const PT S0 = pfma(mpp, c0, pmul(nsc, pmk(tau.a00, tau.a10)));
+                const PT S1 = pfma(mpp, c1, pmul(nsc, pmk(tau.a01, tau.a11)));
+                PT Av = pfma(pbc(-kp.h), pfma(S0, pbc(x), pmul(S1, pbc(y))), pmul(mpp, v));
+                if (kp.ext) {   // wind stress and current of the new cell's node
+                    const V4<Real> f = moved ? G.frc[(uint32_t)cx * (uint32_t)kp.gy + (uint32_t)cy] : fc;
+                    const PT d = psub(pmk(f.x, f.y), v);
+                    const Real cw = kp.rho_w_cd * tsqrt(d.x * d.x + d.y * d.y);
+                    Av = pfma(pbc(kp.ext_impulse), pfma(pbc(cw), d, pmk(f.z, f.w)), Av);
+                }
+                const Real fm = FIXED ? Real(kp.scale_m) : Real(1);
+                const Real fp = FIXED ? Real(kp.scale_p) : Real(1);
+                const PT hp = pbc(kp.h * fp);
+                const PT sA = pmul(Av, pbc(fp)), sS0 = pmul(hp, S0), sS1 = pmul(hp, S1);
+                const Real smp = mp * fm;
+                // Fixed point: a node term is at most max(w) <= 0.5625 times the
+                // bounds below.  Finite sources with |x|, |y| <= 2 raise no P2G
+                // bit; anything else takes the exact tests.
+                const Real lim_p = FIXED ? Real(kp.lim_p) : Real(sizeof(Real) == 4 ? 1e30 : 1e300);
+                const Real lim_m = FIXED ? Real(kp.lim_m) : lim_p;
+                const Real bx = fabs(Av.x) + kp.h * (fabs(S0.x) + fabs(S1.x));
+                const Real by = fabs(Av.y) + kp.h * (fabs(S0.y) + fabs(S1.y));
+                if (!(bx <= lim_p && by <= lim_p && mp <= lim_m && fabs(x) <= Real(2) && fabs(y) <= Real(2))) {
+                    if (FIXED && (!(bx <= Real(kp.lim_p)) || !(by <= Real(kp.lim_p)) || !(mp <= Real(kp.lim_m))))
+                        perr |= kErrFixedOverflow;
+                    Real wxs[3], wys[3];
+                    bspline(x, wxs);
+                    bspline(y, wys);
+                    const Real sw = (wxs[0] + wxs[1] + wxs[2]) + (wys[0] + wys[1] + wys[2]);
+                    if (isnan(sw + smp)) perr |= kErrP2gNanMass;
+                    if (isnan(sw + ((sA.x + sA.y) + (sS0.x + sS1.x) + (sS0.y + sS1.y)))) perr |= kErrP2gNanVel;
+                }
+                V4<Real> a4; a4.x = x; a4.y = y; a4.z = sS1.x; a4.w = sS1.y;
+                sg.A[local] = a4;
+                V4<Real> h4; h4.x = sA.x; h4.y = sA.y; h4.z = sS0.x; h4.w = sS0.y;
+                sg.H[local] = h4;
+                src_key.x = cell;
+                src_key.y = put_src_mass(sg, local, smp);
+                xmn = min(xmn, (unsigned)cx); ymn = min(ymn, (unsigned)cy);
+                xmx = max(xmx, (unsigned)cx); ymx = max(ymx, (unsigned)cy);
+                any = true;
             } else {
                 perr |= kErrLeftArea;
             }
         }
+        sg.K[local] = src_key;
     }
-    // end patches: merge neighbours, then write into the tile.  For int64
-    // accumulators (whose shared atomics are multi-instruction sequences)
-    // the writes go without atomics in two phases (even warps, odd warps)
-    // when warps of one phase touch disjoint nodes and no warp has two
-    // lanes on one cell; float accumulators keep the native atomics.
-    if (!AccOps<Acc>::fixed) {
+    fence_proxy_async_smem();
+
+    // ---- the tile: box of the chunk's scattering cells, +-1 node ------------
+    Tile<Acc, CAP> T;
+    T.t = sm.tile;
+    T.on = false; T.x0 = T.y0 = 0; T.tw = T.th = 0; T.th_rcp = 0;
+    if constexpr (TILE) {
+        {
+            const unsigned FULL = 0xffffffffu;
+            xmn = __reduce_min_sync(FULL, xmn); ymn = __reduce_min_sync(FULL, ymn);
+            xmx = __reduce_max_sync(FULL, xmx); ymx = __reduce_max_sync(FULL, ymx);
+            const unsigned wany = __reduce_or_sync(FULL, any ? 1u : 0u);
+            if (lane == 0) {
+                sm.red[wid][0] = (int)xmn; sm.red[wid][1] = (int)ymn;
+                sm.red[wid][2] = (int)xmx; sm.red[wid][3] = (int)ymx; sm.red[wid][4] = (int)wany;
+            }
+        }
+        __syncthreads();
+        int bx0 = 0xffff, by0 = 0xffff, bx1 = 0, by1 = 0, bany = 0;
+#pragma unroll
+        for (int w = 0; w < NW; w++) {
+            bx0 = min(bx0, sm.red[w][0]); by0 = min(by0, sm.red[w][1]);
+            bx1 = max(bx1, sm.red[w][2]); by1 = max(by1, sm.red[w][3]); bany |= sm.red[w][4];
+        }
+        T.x0 = bx0 - 1; T.y0 = by0 - 1;
+        T.tw = bx1 - bx0 + 3; T.th = by1 - by0 + 3;
+        // 64-bit products: a box spanning the whole grid must not wrap into range
+        T.on = bany && (long long)T.tw * (long long)T.th <= (long long)CAP;
+        if (!T.on) { T.tw = 0; T.th = 0; }
+        T.th_rcp = rcp32(T.th);
+        tile_zero<Acc, CAP, BT>(T);
+        __syncthreads();
+    }
+
+    // ---- phase 2 ----------------------------------------------------------
+    Patch<Real> patch;
+    patch.have = false; patch.in_tile = false; patch.cx = patch.cy = 0;
+#pragma unroll 1
+    for (int j = 0; j < PPT; j++) {
+        const int local = wbase + 32 * j;
+        if (base + (uint32_t)local >= (uint32_t)n) break;
+        const uint2 k2 = sg.K[local];
+        if (k2.x == kNoScatter) continue;
+        const V4<Real> a4 = sg.A[local];
+        const V4<Real> h4 = sg.H[local];
+        SrcP<Real> src;
+        src.cx = (int)(k2.x & 0xffff); src.cy = (int)(k2.x >> 16);
+        src.x = a4.x; src.y = a4.y;
+        src.mp = get_src_mass<Real>(sg, local, k2);
+        src.A = pmk(h4.x, h4.y); src.S0 = pmk(h4.z, h4.w); src.S1 = pmk(a4.z, a4.w);
+        patch_add<Real, Acc, CAP>(patch, src, T, G.acc, kp.gy);
+    }
+    // end patches: merge neighbours, then write them out.  Without a tile
+    // (CAP == 0) every node goes straight to the global accumulators (one
+    // reduction per node and channel).  With a tile: for int64 accumulators
+    // (whose shared atomics are multi-instruction sequences) the writes go
+    // without atomics in two phases (even warps, odd warps) when warps of one
+    // phase touch disjoint nodes and no warp has two lanes on one cell; float
+    // accumulators keep the native atomics.
+    if constexpr (!TILE) {
+        bool low = true, high = true;
+        patch_merge(patch, lane, low, high, false);
+        if (patch.have) {
+#pragma unroll
+            for (int a = 0; a < 3; a++)
+#pragma unroll
+                for (int b = 0; b < 3; b++)
+                    if ((b != 0 || low) && (b != 2 || high)) patch_node<Real, Acc, CAP>(patch, T, G.acc, kp.gy, a, b);
+        }
+        // one stage: every thread has read its entries; refill the stage
+        if (STAGES == 1) {
+            __syncthreads();
+            if (tid == 0 && next) fetch_chunk(sm.stage[0], Pn, base_n, CH, &sm.mbar[0]);
+        }
+        return;
+    } else if (!FIXED) {
         bool low = true, high = true;
         patch_merge(patch, lane, low, high);
         if (patch.have) {
@@ -1062,9 +1193,11 @@ __device__ __forceinline__ void fused_chunk(ChunkSmem<Real, Acc, BT, PPT, CAP, S
         }
         __syncthreads();
     }
-    // one stage: its points are all read now, fetch the next chunk into it
-    if (STAGES == 1 && tid == 0 && next) fetch_chunk(sm.stage[0], Pn, base_n, CH, &sm.mbar[0]);
-    tile_flush<Acc, CAP, BT>(T, G.acc, kp.gx, kp.gy);
+    if constexpr (TILE) {
+        // one stage: its entries are all read now, fetch the next chunk into it
+        if (STAGES == 1 && tid == 0 && next) fetch_chunk(sm.stage[0], Pn, base_n, CH, &sm.mbar[0]);
+        tile_flush<Acc, CAP, BT>(T, G.acc, kp.gx, kp.gy);
+    }
 }
 
 template <class Real, class Acc, int BT, int PPT, int CAP, int STAGES, bool HARVEST>

@@ -36,7 +36,8 @@ public:
     static constexpr int BT = sizeof(Real) == 8 ? 128 : ICEMPM_FUSED_BT;
     static constexpr int PPT = sizeof(Real) == 8 ? 2 : ICEMPM_FUSED_PPT;
     static constexpr int CH = BT * PPT;
-    static constexpr int CAP = ICEMPM_FUSED_CAP;     // nodes in the shared scatter tile
+    static constexpr int CAP = ICEMPM_FUSED_CAP;     // nodes in the fused kernel's shared scatter tile (0: none)
+    static constexpr int CAP_P2G = 512;              // nodes in the priming scatter's shared tile
     static constexpr int BT_P2G = 256;   // threads per CTA of the priming scatter
     static constexpr int GRAPH_STEPS = 32;
     static constexpr size_t PAD = 2048;  // point arrays are padded to whole chunks
@@ -399,7 +400,7 @@ public:
         ICEMPM_CUDA(cudaMemsetAsync(&st_->err_pending, 0, sizeof(uint32_t), stream_));
         if (n_ > 0) {
             const unsigned nb = (n_ + BT_P2G - 1) / BT_P2G;
-            k_p2g<Real, Acc, BT_P2G, CAP><<<nb, BT_P2G, 0, stream_>>>(kp_, pts_[par_], grid(), st_, (int)n_);
+            k_p2g<Real, Acc, BT_P2G, CAP_P2G><<<nb, BT_P2G, 0, stream_>>>(kp_, pts_[par_], grid(), st_, (int)n_);
             launches_++;
             ICEMPM_CUDA(cudaGetLastError());
         }

@@ -3,9 +3,11 @@
 in numpy, float64 sums (test infrastructure: the checker of the GPU frame
 kernels, never on the product path).
 
-Parity unpinned: the reference function belongs to the snapshot manager,
-which needs HDF5, OpenJPEG and the whole Model to compile, so it cannot be run
-here; this restatement follows its source line by line:
+Pinned: tests/test_frame.py checks it against the golden fixture
+tests/golden/frame_ridging.npz, the output of the reference function itself
+(compiled from the checkout by oracle/refbuild/build_ref.py build_frame, with
+stand-ins for the rest of the Model); the reference sums in float32 in point
+order, this restatement in float64.  It follows the source line by line:
   * enabled points only (utility without 0x20000);
   * quadratic B-spline weights of the cell-local position (CalculateWeightCoeffs,
     snapshotmanager.cpp:611-620), nodes (x+i)*GridY + (y+j), i, j in -1..1;

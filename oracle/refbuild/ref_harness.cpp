@@ -3,10 +3,13 @@
  *   parameters_sim.cpp, hssoa/host_side_soa.cpp, hssoa/proxypoint2d.cpp
  * compiled unmodified, where they lie, by oracle/refbuild/build_ref.py, with
  * the stand-in headers in stubs/.  The three __global__ kernels run as plain
- * functions, once per (block, thread); P2G runs serially in index order, so
- * its "atomics" are applied in point-index order; the grid update and G2P
- * run their blocks in parallel.  TEST INFRASTRUCTURE ONLY: it pins the
- * oracle restatement (oracle/icempm_oracle.c) to the reference code. */
+ * functions, once per (block, thread).  ref_run_steps runs P2G serially in
+ * index order, so its "atomics" are applied in point-index order (the golden
+ * fixtures); ref_run_steps_parallel runs P2G's blocks in parallel with real
+ * atomic adds, as the GPU does (the timed host baseline).  The grid update
+ * and G2P always run their blocks in parallel.  TEST INFRASTRUCTURE ONLY: it
+ * pins the oracle restatement (oracle/icempm_oracle.c) to the reference code
+ * and times the reference's own step on the host cores. */
 #include <cstddef>
 #include <cstdint>
 #include <cstring>
@@ -18,6 +21,7 @@
 #include "helper_math.cuh"
 
 thread_local ref_dim3 blockIdx, threadIdx, blockDim;
+bool ref_atomics_on = false;
 
 /* prototypes of the kernel helpers, same signatures as gpu_partition.h:28-59 */
 __device__ void svd2x2(const PointMatrix2r &mA, PointMatrix2r &mU, PointVector2r &mS, PointMatrix2r &mV);
@@ -112,9 +116,11 @@ void ref_svd2x2(const double *F, double *U, double *S, double *V)
 
 /* The sub-step loop of Model::Step (model.cpp:18-39) over GPU_Partition's
  * reset_grid / p2g / update_nodes / g2p (gpu_partition.cpp:300-365) with the
- * reference kernels.  Returns gpu_error_indicator; adds to *disabled. */
-uint32_t ref_run_steps(const SimParams *prms, double *soa, size_t pitch, size_t n, double *grid,
-                       size_t gpitch, uint8_t *status, int nsteps, int first_step, int *disabled)
+ * reference kernels.  parallel_p2g: P2G's blocks over OpenMP threads with
+ * atomic adds (summation order then varies run to run, as on the GPU).
+ * Returns gpu_error_indicator; adds to *disabled. */
+static uint32_t run_steps(const SimParams *prms, double *soa, size_t pitch, size_t n, double *grid, size_t gpitch,
+                          uint8_t *status, int nsteps, int first_step, int *disabled, bool parallel_p2g)
 {
     gprms = *prms;
     partition_buffer_pts = soa;
@@ -126,18 +132,33 @@ uint32_t ref_run_steps(const SimParams *prms, double *soa, size_t pitch, size_t 
     partition_grid_status = status;
     gpu_error_indicator = 0;
     gpu_disabled_points_count = 0;
+    ref_atomics_on = parallel_p2g;
     const size_t nNodes = (size_t)prms->GridXTotal * prms->GridYTotal;
     for (int k = 0; k < nsteps; k++) {
         const int step = first_step + k;
         const float simulation_time = (float)(prms->InitialTimeStep * step);
         std::memset(grid, 0, gpitch * 3 * sizeof(double));
-        emulate_launch(n, prms->tpb_P2G, [] { partition_kernel_p2g(); });
+        if (parallel_p2g) emulate_launch_parallel(n, prms->tpb_P2G, [] { partition_kernel_p2g(); });
+        else emulate_launch(n, prms->tpb_P2G, [] { partition_kernel_p2g(); });
         emulate_launch_parallel(nNodes, prms->tpb_Upd, [&] { partition_kernel_update_nodes(simulation_time); });
         const bool isCycleStart = step % prms->UpdateEveryNthStep == 0;
         emulate_launch_parallel(n, prms->tpb_G2P, [&] { partition_kernel_g2p(isCycleStart); });
     }
+    ref_atomics_on = false;
     if (disabled) *disabled += gpu_disabled_points_count;
     return gpu_error_indicator;
+}
+
+uint32_t ref_run_steps(const SimParams *prms, double *soa, size_t pitch, size_t n, double *grid,
+                       size_t gpitch, uint8_t *status, int nsteps, int first_step, int *disabled)
+{
+    return run_steps(prms, soa, pitch, n, grid, gpitch, status, nsteps, first_step, disabled, false);
+}
+
+uint32_t ref_run_steps_parallel(const SimParams *prms, double *soa, size_t pitch, size_t n, double *grid,
+                                size_t gpitch, uint8_t *status, int nsteps, int first_step, int *disabled)
+{
+    return run_steps(prms, soa, pitch, n, grid, gpitch, status, nsteps, first_step, disabled, true);
 }
 
 /* HostSideSOA::RemoveDisabledAndSort on a caller-owned buffer. */

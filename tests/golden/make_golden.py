@@ -12,6 +12,8 @@ the committed .npz files are what the tests read.
 Stored per fixture: the SimParams bytes, grid status, current field, the input
 HSSOA, the number of steps and first step index, the output HSSOA, the output
 grid (mass/velocity rows after the last step), error bits and disabled count.
+frame_ridging holds the reference's PrepareFrameArrays output instead (see
+frame_fixture).
 """
 import ctypes as C
 import os
@@ -85,6 +87,35 @@ def main():
          extra=dict(sorted_soa=sorted_soa, sorted_n=np.int64(m)))
     z, _ = load("disable_then_sort")
     assert int(z["disabled"]) > 0 and int(z["sorted_n"]) == n - int(z["disabled"]), (int(z["disabled"]), int(z["sorted_n"]))
+    frame_fixture()
+
+
+def frame_fixture():
+    """frame_ridging: the saved-frame arrays of the reference's own
+    SnapshotManager::PrepareFrameArrays (snapshotmanager.cpp:623-765, compiled
+    by oracle/refbuild/build_ref.py build_frame) for a ridging scene advanced
+    20 steps by the reference kernels, with 5% of the points disabled, random
+    point colours, the reference's grid status and seeded boundary forces."""
+    sc = scenes.ridging(seed=15, gx=96, gy=64, cells_x=40, cells_y=30, speed=2.0)
+    rng = np.random.default_rng(15)
+    soa = sc.soa.copy()
+    n, G = sc.n, sc.grid_nodes
+    util = H.get_u32(soa, IDX_UTILITY, n).copy()
+    util[rng.random(n) < 0.05] |= STATUS_DISABLED
+    H.set_u32(soa, IDX_UTILITY, util, n)
+    grid = _grid(sc)
+    err, dis = build_ref.run_steps(sc.prms, soa, n, grid, sc.status, 20, 0)
+    colors = rng.integers(0, 1 << 24, n).astype(np.uint32)
+    forces = rng.normal(0.0, 50.0, 2 * G)
+    out = build_ref.prepare_frame(sc.prms, soa, n, sc.status, forces, colors)
+    d = dict(prms=np.frombuffer(bytes(sc.prms), np.uint8), status=sc.status, soa=soa, n=np.int64(n),
+             colors=colors, forces=forces, err=np.uint32(err))
+    d.update({"out_" + k: v for k, v in out.items()})
+    np.savez_compressed(os.path.join(HERE, "frame_ridging.npz"), **d)
+    print(f"frame_ridging: n={n} nodes={G} masked={int(out['mass_mask'].sum())} err={err:#x}")
 
 if __name__ == "__main__":
-    main()
+    if sys.argv[1:] == ["frame"]:
+        frame_fixture()
+    else:
+        main()

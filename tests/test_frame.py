@@ -1,18 +1,78 @@
-"""Saved-frame grid arrays (icempm_prepare_frame) against the CPU restatement
-of SnapshotManager::PrepareFrameArrays (oracle/frame_reference.py).
+"""Saved-frame grid arrays (icempm_prepare_frame) against the reference's own
+SnapshotManager::PrepareFrameArrays (the golden fixture frame_ridging, made by
+tests/golden/make_golden.py from the reference function compiled by
+oracle/refbuild/build_ref.py) and against the CPU restatement
+(oracle/frame_reference.py), which the same fixture pins.
 
 Tolerances: the ten channels within 1e-4 of each channel's largest magnitude
 (FP32 sums in another order), Jpinv (an average of values near 1, minus 1)
 within 2e-6 absolute; mass mask and points per cell identical except
 nodes whose density sits within 1e-5 of the 0.1 threshold; colour within one
 unit (truncation after FP32 blending); region forces within 1e-4 relative.
+The restatement (float64 sums) against the reference (float32 sums in point
+order): channels within 1e-5 of the channel's largest magnitude.
 """
+import os
+
 import numpy as np
 import pytest
 
 from icempm_2d_sp_b200 import scenes, hssoa as H
 from icempm_2d_sp_b200.params import Options, SimParams, IDX_UTILITY, STATUS_DISABLED
 from oracle import frame_reference as fr
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "frame_ridging.npz")
+CHANNELS = ("density", "mass", "vx", "vy", "Jpinv", "P", "Q", "r", "g", "b")
+
+
+def _golden():
+    z = np.load(GOLDEN)
+    return z, SimParams.from_buffer_copy(z["prms"].tobytes())
+
+
+def _compare(got, z, tol_rel, jp_abs, forces=True):
+    for k in CHANNELS:
+        ref = z["out_" + k].astype(np.float64)
+        tol = jp_abs if k == "Jpinv" else tol_rel * max(np.abs(ref).max(), 1e-30)
+        assert np.abs(np.asarray(got[k], np.float64) - ref).max() <= tol, k
+    dens = z["out_density"].astype(np.float64)
+    border = np.abs(dens - 0.1) < 1e-5
+    assert np.array_equal(np.asarray(got["mass_mask"])[~border], z["out_mass_mask"][~border])
+    assert np.array_equal(np.asarray(got["count"]), z["out_count"])
+    assert np.abs(np.asarray(got["rgb"]).astype(int) - z["out_rgb"].astype(int)).max() <= 1
+    if forces:
+        rf = z["out_forces_per_region"].astype(np.float64).reshape(-1)
+        gf = np.asarray(got["forces_per_region"], np.float64).reshape(-1)
+        assert np.abs(gf - rf).max() <= tol_rel * max(np.abs(rf).max(), 1e-30)
+
+
+def test_restatement_matches_reference_golden():
+    """The CPU restatement reproduces the reference function's own output."""
+    z, prms = _golden()
+    n = int(z["n"])
+    assert int(z["out_mass_mask"].sum()) > 0 and np.abs(z["out_forces_per_region"]).max() > 0
+    out = fr.prepare_frame(prms, z["soa"], n, z["status"], z["forces"], z["colors"])
+    _compare(out, z, 1e-5, 1e-6)
+
+
+@pytest.mark.gpu
+def test_frame_arrays_match_reference_golden():
+    """icempm_prepare_frame on the fixture's point state (uploaded through the
+    C ABI, no sub-steps: the force accumulator is empty, so the region forces
+    are zero) against the reference function's arrays."""
+    from icempm_2d_sp_b200 import capi
+    capi.load()
+    if capi.device_count() < 1:
+        pytest.fail("no CUDA device visible to the library")
+    z, prms = _golden()
+    n = int(z["n"])
+    G = prms.GridXTotal * prms.GridYTotal
+    with capi.Context(prms, z["status"], np.zeros(2 * G), capacity=n, options=Options.default()) as ctx:
+        ctx.upload(z["soa"], n)
+        ctx.clear_force_accumulator()
+        got = ctx.prepare_frame(1, z["colors"])
+    _compare(got, z, 1e-4, 2e-6, forces=False)
+    assert np.abs(got["forces_per_region"]).max() == 0.0
 
 
 def test_reference_restatement_single_point():

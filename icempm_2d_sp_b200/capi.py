@@ -25,7 +25,7 @@ EXPORTS = [
     "icempm_mlp_param_count", "icempm_mlp_grad", "icempm_mlp_adam", "icempm_mlp_forward", "icempm_return_map_exact",
     "icempm_return_map_learned", "icempm_harvest_begin", "icempm_harvest_end", "icempm_prepare_frame",
     "icempm_set_flow_frames", "icempm_set_wind_frames", "icempm_set_forcing_time", "icempm_get_forcing",
-    "icempm_download_points_async", "icempm_download_wait",
+    "icempm_download_points_async", "icempm_download_wait", "icempm_debug_barrier_timeout",
 ]
 
 FRAME_CHANNELS = ("point_density", "mass", "vx", "vy", "Jpinv", "P", "Q", "r", "g", "b")
@@ -84,6 +84,7 @@ def load(path: str = LIB_PATH):
         "icempm_download_points": (C.c_int, [h, dp, C.c_uint32, C.POINTER(C.c_uint32)]),
         "icempm_download_points_async": (C.c_int, [h, dp, C.c_uint32, C.POINTER(C.c_uint32)]),
         "icempm_download_wait": (C.c_int, [h]),
+        "icempm_debug_barrier_timeout": (C.c_int, [h, C.c_uint32, C.c_uint32]),
         "icempm_get_status": (C.c_int, [h, C.POINTER(C.c_uint32), C.POINTER(C.c_int32)]),
         "icempm_clear_force_accumulator": (C.c_int, [h]),
         "icempm_get_boundary_forces": (C.c_int, [h, dp, C.c_int32]),
@@ -291,6 +292,12 @@ class Context:
     def download_wait(self):
         check(self._L.icempm_download_wait(self.h))
         self._pending = None
+
+    def debug_barrier_timeout(self, extra_bytes: int, wait_limit_us: int):
+        """Test hook: make the fused kernel's chunk barriers expect extra_bytes
+        more than their copies deliver, with a wait limit of wait_limit_us
+        ((0, 0) restores the production setting)."""
+        check(self._L.icempm_debug_barrier_timeout(self.h, int(extra_bytes), int(wait_limit_us)))
 
     def status(self) -> tuple:
         e, d = C.c_uint32(0), C.c_int32(0)

@@ -16,10 +16,11 @@ template <class Real, class Acc>
 class BatchT final : public Batch {
     using E = EngineT<Real, Acc>;
     static constexpr int BT = E::BT, PPT = E::PPT, CH = E::CH;
-    // shapes of the batched fused kernel the tuner chooses from: tile nodes x stages
-    static constexpr int NSHAPES = 3;
-    static constexpr int SHAPE_TILE[NSHAPES] = {512, 1024, 512};
-    static constexpr int SHAPE_STAGES[NSHAPES] = {1, 1, 2};
+    // shapes of the batched fused kernel the tuner chooses from: tile nodes
+    // (0: no shared tile, node sums straight to the global accumulators) x stages
+    static constexpr int NSHAPES = 4;
+    static constexpr int SHAPE_TILE[NSHAPES] = {0, 0, 512, 1024};
+    static constexpr int SHAPE_STAGES[NSHAPES] = {2, 1, 1, 1};
 
     template <int CAPX, int ST> using Smem = ChunkSmem<Real, Acc, BT, PPT, CAPX, ST>;
 
@@ -39,9 +40,10 @@ public:
         ICEMPM_CUDA(cudaMalloc(&d_scenes_, eng_.size() * sizeof(SceneDesc<Real, Acc>)));
         int sms = 0;
         ICEMPM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_));
-        int rc = setup_shape<512, 1>(0, sms);
-        if (!rc) rc = setup_shape<1024, 1>(1, sms);
-        if (!rc) rc = setup_shape<512, 2>(2, sms);
+        int rc = setup_shape<0, 2>(0, sms);
+        if (!rc) rc = setup_shape<0, 1>(1, sms);
+        if (!rc) rc = setup_shape<512, 1>(2, sms);
+        if (!rc) rc = setup_shape<1024, 1>(3, sms);
         if (rc) return rc;
         if (ctas_[0] < 1) return fail(ICEMPM_E_UNSUPPORTED, "batched fused kernel does not fit on one SM");
         ICEMPM_CUDA(cudaStreamSynchronize(stream_));
@@ -152,7 +154,7 @@ public:
         int shape = -1;
         for (int s = 0; s < NSHAPES; s++)
             if (SHAPE_TILE[s] == t->tile_nodes && SHAPE_STAGES[s] == t->stages) shape = s;
-        if (shape < 0) return fail(ICEMPM_E_UNSUPPORTED, "tile_nodes/stages: 512/1, 1024/1 or 512/2");
+        if (shape < 0) return fail(ICEMPM_E_UNSUPPORTED, "tile_nodes/stages: 0/2, 0/1, 512/1 or 1024/1");
         if (ctas_[shape] < 1) return fail(ICEMPM_E_UNSUPPORTED, "that kernel shape does not fit on this device");
         if (t->sort_every < 0 || t->graph_steps < 0) return fail(ICEMPM_E_ARG, "negative cadence");
         if (shape != shape_ || t->graph_steps != tune_.graph_steps) invalidate_graph();
@@ -200,6 +202,8 @@ private:
             E *e = eng_[i];
             SceneDesc<Real, Acc> &s = d[i];
             s.kp = e->kp_;
+            s.kp.tx_extra = 0;                  // the batch kernel waits for the exact bytes, 1 s at most
+            s.kp.wait_ns = kWaitLimitNs;
             s.P = e->pts_[e->par_];
             s.G = e->grid();
             s.st = e->st_;
@@ -265,9 +269,10 @@ private:
         if (nblocks_ > 0)
             k_grid_update_batch<Real, Acc><<<nblocks_, 256, 0, stream_>>>(d_scenes_, d_block_scene_, bst_);
         if (nchunks_ > 0) {
-            if (shape_ == 0) launch_fused<512, 1>();
-            else if (shape_ == 1) launch_fused<1024, 1>();
-            else launch_fused<512, 2>();
+            if (shape_ == 0) launch_fused<0, 2>();
+            else if (shape_ == 1) launch_fused<0, 1>();
+            else if (shape_ == 2) launch_fused<512, 1>();
+            else launch_fused<1024, 1>();
         }
         launches_ += 2;
     }
@@ -322,7 +327,7 @@ private:
     std::vector<int> chunk_scene_, block_scene_;
     int ctas_[NSHAPES] = {0, 0, 0};
     int shape_ = 0;
-    icempm_batch_tuning_t tune_{512, 1, 0, 50, 0.0f, {0, 0, 0}};
+    icempm_batch_tuning_t tune_{0, 2, 0, 50, 0.0f, {0, 0, 0}};
     int since_sort_ = 0;
     bool timed_ = false;
     cudaGraphExec_t graph_exec_ = nullptr;

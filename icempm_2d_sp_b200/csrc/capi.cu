@@ -300,6 +300,13 @@ int icempm_harvest_end(icempm_t *ctx, float *records, uint32_t capacity, uint32_
     ICEMPM_TRY(ctx->eng->harvest_end(records, capacity, count));
 }
 
+int icempm_debug_barrier_timeout(icempm_t *ctx, uint32_t extra_bytes, uint32_t wait_limit_us)
+{
+    if (extra_bytes % 16u != 0) return fail(ICEMPM_E_ARG, "extra_bytes must be a multiple of 16");
+    ICEMPM_GUARD_CTX(ctx);
+    ICEMPM_TRY(ctx->eng->set_barrier_test(extra_bytes, wait_limit_us));
+}
+
 int icempm_batch_create(icempm_t *const *contexts, int32_t count, icempm_batch_t **out)
 {
     if (!out) return fail(ICEMPM_E_ARG, "out is null");

@@ -45,8 +45,9 @@
 #include "icempm.h"
 
 // Shape of the FP32-state fused kernel: threads per CTA, points per thread,
-// nodes of the shared scatter tile, CTAs per SM it is compiled for (this
-// caps registers at 96: occupancy is what hides its latencies).
+// nodes of the shared scatter tile (0: no tile, each warp's merged node sums
+// go straight to the global accumulators), CTAs per SM it is compiled for
+// (this caps registers at 96: occupancy is what hides its latencies).
 #ifndef ICEMPM_FUSED_BT
 #define ICEMPM_FUSED_BT 128
 #endif
@@ -54,16 +55,19 @@
 #define ICEMPM_FUSED_PPT 4
 #endif
 #ifndef ICEMPM_FUSED_CAP
-#define ICEMPM_FUSED_CAP 512
+#define ICEMPM_FUSED_CAP 0
 #endif
 #ifndef ICEMPM_FUSED_MINB
 #define ICEMPM_FUSED_MINB 5
 #endif
 // Stages of point state in shared memory (2: the next chunk is fetched while
-// this one is computed; 1: it is fetched while this one's tile is flushed,
-// which leaves room for more CTAs per SM).
+// this one is computed; 1: it is fetched at the end of this one).
 #ifndef ICEMPM_FUSED_STAGES
-#define ICEMPM_FUSED_STAGES 1
+#define ICEMPM_FUSED_STAGES 2
+#endif
+// Nodes per thread of the grid update (1, 2 or 4; vector loads and stores).
+#ifndef ICEMPM_UPDATE_NPT
+#define ICEMPM_UPDATE_NPT 2
 #endif
 // 1: the fused kernel keeps the 3x3 node velocities of the last cell in
 // registers for the thread's next point; 0: it loads them for every point.
@@ -187,6 +191,8 @@ template <class Real> struct KParams {
     MatT<Real> mat;
     HarvestBuf *harvest;            // return-map pairs are recorded when not null
     int harvest_stride;             // ... for points with (index + step) % stride == 0
+    uint32_t tx_extra;              // bytes each chunk's barrier expects beyond its copies (0; tests of the timeout)
+    unsigned long long wait_ns;     // time limit of a barrier wait
 };
 
 // Fire-and-forget reductions into global memory (red.global: no value comes
@@ -526,14 +532,95 @@ __device__ __forceinline__ void fold_pending(DevStatus *st)
     if (pe) { atomicOr(&st->err, pe); st->err_pending = 0; }
 }
 
+// Velocity of a node whose accumulators (am, apx, apy) are not all zero, from
+// its status byte (grid_update_node after its loads); adds the wall reaction
+// into the force accumulator and error bits into err.
 template <class Real, class Acc, bool EXT>
+__device__ __forceinline__ V2<Real> node_velocity(const KParams<Real> &kp, const Grid<Real, Acc> &G, long long idx,
+                                                  int step, Acc am, Acc apx, Acc apy, uint8_t status, uint32_t &err)
+{
+    V2<Real> out;
+    out.x = Real(0); out.y = Real(0);
+    const Real mass = AccOps<Acc>::template to<Real>(am, kp.inv_scale_m);
+    if (mass != Real(0)) {
+        const Real mx = AccOps<Acc>::template to<Real>(apx, kp.inv_scale_p);
+        const Real my = AccOps<Acc>::template to<Real>(apy, kp.inv_scale_p);
+        Real vx = mx / mass, vy = my / mass;
+        if (status != 100) {
+            vx = Real(0); vy = Real(0);
+            double2 f = G.force[idx];
+            f.x += double(mx); f.y += double(my);
+            G.force[idx] = f;
+        } else if (!EXT) {
+            const V2<Real> c = G.cur[idx];
+            const double t = (double)(float)(kp.dt_d * (double)step);
+            const double ramp = (t < 300000) ? 1 + fmin(t / (3600 * 2), 2.) : 3 + fmin((t - 300000) / (3600 * 10), 2.);
+            const Real wx = c.x * Real(ramp), wy = c.y * Real(ramp);
+            const Real ux = wx - vx, uy = wy - vy;
+            const Real um = tsqrt(ux * ux + uy * uy);
+            Real k = Real(kp.kL) + Real(kp.kQ) * um;
+            k = fmin(k, Real(0.1));
+            vx += k * ux; vy += k * uy;
+        }
+        if (vx * vx + vy * vy > kp.vmax2_01) { vx = Real(0); vy = Real(0); }
+        if (isnan(vx) || isnan(vy)) err |= kErrGridNan;
+        out.x = vx; out.y = vy;
+    }
+    return out;
+}
+
+// NPT consecutive values of T as one aligned vector (16-byte loads and stores).
+template <class T, int NPT> struct alignas(sizeof(T) * NPT >= 16 ? 16 : sizeof(T) * NPT) VecN { T v[NPT]; };
+
+// NPT consecutive nodes per thread: the three accumulator channels, the
+// status bytes and the velocities move as vectors, so more bytes are in
+// flight per thread (the one-node form waits on each load).  Channel arrays
+// must start 16-byte aligned (the context pads each to a multiple of 32
+// nodes); the last partial group takes the one-node path.
+template <class Real, class Acc, bool EXT, int NPT>
 __global__ void __launch_bounds__(256) k_grid_update(KParams<Real> kp, Grid<Real, Acc> G, DevStatus *st,
                                                      long long nnodes)
 {
-    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx == 0) fold_pending(st);
-    if (idx >= nnodes) return;
-    grid_update_node<Real, Acc, EXT>(kp, G, st, idx, st->step);
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t == 0) fold_pending(st);
+    const long long i0 = t * NPT;
+    if (i0 >= nnodes) return;
+    const int step = st->step;
+    if (NPT == 1 || i0 + NPT > nnodes) {
+        for (long long idx = i0; idx < nnodes && idx < i0 + NPT; idx++) grid_update_node<Real, Acc, EXT>(kp, G, st, idx, step);
+        return;
+    }
+    using AV = VecN<Acc, NPT>;
+    const AV m = *reinterpret_cast<const AV *>(G.acc.m + i0);
+    const AV px = *reinterpret_cast<const AV *>(G.acc.px + i0);
+    const AV py = *reinterpret_cast<const AV *>(G.acc.py + i0);
+    bool nz[NPT], any = false;
+#pragma unroll
+    for (int k = 0; k < NPT; k++) {
+        nz[k] = m.v[k] != Acc(0) || px.v[k] != Acc(0) || py.v[k] != Acc(0);
+        any |= nz[k];
+    }
+    VecN<V2<Real>, NPT> vel;
+    uint32_t err = 0;
+    if (any) {
+        AV z;
+#pragma unroll
+        for (int k = 0; k < NPT; k++) z.v[k] = Acc(0);
+        *reinterpret_cast<AV *>(G.acc.m + i0) = z;
+        *reinterpret_cast<AV *>(G.acc.px + i0) = z;
+        *reinterpret_cast<AV *>(G.acc.py + i0) = z;
+        const VecN<uint8_t, NPT> stv = *reinterpret_cast<const VecN<uint8_t, NPT> *>(G.status + i0);
+#pragma unroll
+        for (int k = 0; k < NPT; k++) {
+            vel.v[k].x = Real(0); vel.v[k].y = Real(0);
+            if (nz[k]) vel.v[k] = node_velocity<Real, Acc, EXT>(kp, G, i0 + k, step, m.v[k], px.v[k], py.v[k], stv.v[k], err);
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < NPT; k++) { vel.v[k].x = Real(0); vel.v[k].y = Real(0); }
+    }
+    *reinterpret_cast<VecN<V2<Real>, NPT> *>(G.vel + i0) = vel;
+    if (err) atomicOr(&st->err, err);
 }
 
 // ---- fused G2P (step k) + P2G (step k+1) -----------------------------------
@@ -584,14 +671,16 @@ __device__ __forceinline__ unsigned long long global_ns()
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
     return t;
 }
-// Gives up after 2^24 polls or 1 s, whichever comes first.
-__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long *bar, uint32_t parity)
+// Gives up after 2^24 polls or limit_ns, whichever comes first.
+constexpr unsigned long long kWaitLimitNs = 1000000000ull;
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long *bar, uint32_t parity,
+                                                  unsigned long long limit_ns = kWaitLimitNs)
 {
     if (mbar_try_wait(bar, parity)) return true;
     const unsigned long long t0 = global_ns();
     for (uint32_t k = 0; k < (1u << 24); k++) {
         if (mbar_try_wait(bar, parity)) return true;
-        if ((k & 255u) == 255u && global_ns() - t0 > 1000000000ull) return false;
+        if ((k & 255u) == 255u && global_ns() - t0 > limit_ns) return false;
     }
     return false;
 }
@@ -801,13 +890,16 @@ template <class Real> __device__ __forceinline__ P2<Real> ld_vel(const V2<Real> 
     return *reinterpret_cast<const P2<Real> *>(p);
 }
 
+// Issues the bulk copies of one chunk's A, H, K into a stage; the barrier
+// expects their bytes plus `extra` (0 except in tests of the timeout path,
+// where the wait then runs out although every copy has landed).
 template <class Real, class Stage>
 __device__ __forceinline__ void fetch_chunk(Stage &sg, const Pts<Real> &P, uint32_t base, int ch,
-                                            unsigned long long *bar)
+                                            unsigned long long *bar, uint32_t extra = 0u)
 {
     const uint32_t bv = (uint32_t)ch * (uint32_t)sizeof(V4<Real>);
     const uint32_t bk = (uint32_t)ch * (uint32_t)sizeof(uint2);
-    mbar_arrive_expect_tx(bar, 2 * bv + bk);
+    mbar_arrive_expect_tx(bar, 2 * bv + bk + extra);
     bulk_to_smem(sg.A, P.A + base, bv, bar);
     bulk_to_smem(sg.H, P.H + base, bv, bar);
     bulk_to_smem(sg.K, P.K + base, bk, bar);
@@ -1144,7 +1236,7 @@ __device__ __forceinline__ void fused_chunk(ChunkSmem<Real, Acc, BT, PPT, CAP, S
         // one stage: every thread has read its entries; refill the stage
         if (STAGES == 1) {
             __syncthreads();
-            if (tid == 0 && next) fetch_chunk(sm.stage[0], Pn, base_n, CH, &sm.mbar[0]);
+            if (tid == 0 && next) fetch_chunk(sm.stage[0], Pn, base_n, CH, &sm.mbar[0], kp.tx_extra);
         }
         return;
     } else if (!FIXED) {
@@ -1195,7 +1287,7 @@ __device__ __forceinline__ void fused_chunk(ChunkSmem<Real, Acc, BT, PPT, CAP, S
     }
     if constexpr (TILE) {
         // one stage: its entries are all read now, fetch the next chunk into it
-        if (STAGES == 1 && tid == 0 && next) fetch_chunk(sm.stage[0], Pn, base_n, CH, &sm.mbar[0]);
+        if (STAGES == 1 && tid == 0 && next) fetch_chunk(sm.stage[0], Pn, base_n, CH, &sm.mbar[0], kp.tx_extra);
         tile_flush<Acc, CAP, BT>(T, G.acc, kp.gx, kp.gy);
     }
 }
@@ -1218,7 +1310,7 @@ k_g2p_p2g(KParams<Real> kp, Pts<Real> P, Grid<Real, Acc> G, DevStatus *st, int n
     }
     __syncthreads();
     int c = blockIdx.x;
-    if (tid == 0 && c < nchunks) fetch_chunk(sm.stage[0], P, (uint32_t)c * CH, CH, &sm.mbar[0]);
+    if (tid == 0 && c < nchunks) fetch_chunk(sm.stage[0], P, (uint32_t)c * CH, CH, &sm.mbar[0], kp.tx_extra);
 
     const int step = st->step;
     const bool recordPQ = kp.update_every > 0 && (step % kp.update_every) == 0;
@@ -1229,11 +1321,20 @@ k_g2p_p2g(KParams<Real> kp, Pts<Real> P, Grid<Real, Acc> G, DevStatus *st, int n
     for (int it = 0; c < nchunks; it++, c += (int)gridDim.x) {
         const int s = STAGES == 2 ? (it & 1) : 0;
         const uint32_t parity = STAGES == 2 ? ((uint32_t)(it >> 1) & 1u) : ((uint32_t)it & 1u);
-        const bool ok = mbar_wait_bounded(&sm.mbar[s], parity);
-        if (__syncthreads_or(!ok)) { err |= kErrBarrierTimeout; break; }
+        const bool ok = mbar_wait_bounded(&sm.mbar[s], parity, kp.wait_ns);
+        if (__syncthreads_or(!ok)) {
+            // the chunk's copies did not complete in time: report it, give
+            // copies still in flight one more bounded wait to land in this
+            // CTA's shared memory, and leave
+            err |= kErrBarrierTimeout;
+            if (tid == 0) (void)mbar_wait_bounded(&sm.mbar[s], parity, kp.wait_ns);
+            __syncthreads();
+            break;
+        }
         const bool next = c + (int)gridDim.x < nchunks;
         const uint32_t base_n = (uint32_t)(c + (int)gridDim.x) * CH;
-        if (STAGES == 2 && tid == 0 && next) fetch_chunk(sm.stage[s ^ 1], P, base_n, CH, &sm.mbar[s ^ 1]);
+        if (STAGES == 2 && tid == 0 && next)
+            fetch_chunk(sm.stage[s ^ 1], P, base_n, CH, &sm.mbar[s ^ 1], kp.tx_extra);
         fused_chunk<Real, Acc, BT, PPT, CAP, STAGES, HARVEST>(sm, s, kp, P, G, (uint32_t)c * CH, n, step, recordPQ, store_vc,
                                                      next, P, base_n, err, perr, ndis);
     }
@@ -1330,6 +1431,8 @@ k_g2p_p2g_batch(const SceneDesc<Real, Acc> *__restrict__ scenes, const int *__re
         const bool ok = mbar_wait_bounded(&sm.mbar[s], parity);
         if (__syncthreads_or(!ok)) {
             warp_flush_status(S.st, kErrBarrierTimeout, 0u, 0);
+            if (tid == 0) (void)mbar_wait_bounded(&sm.mbar[s], parity);
+            __syncthreads();
             break;
         }
         const int cn = c + (int)gridDim.x;

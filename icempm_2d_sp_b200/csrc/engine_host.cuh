@@ -85,14 +85,15 @@ public:
             P.pid = (uint32_t *)take(nc * sizeof(uint32_t));
         }
         // grid
-        ICEMPM_CUDA(cudaMalloc(&acc_, 3 * G_ * sizeof(Acc)));
+        Gp_ = (G_ + 31) / 32 * 32;   // channel stride: every channel starts 256-byte aligned
+        ICEMPM_CUDA(cudaMalloc(&acc_, 3 * Gp_ * sizeof(Acc)));
         ICEMPM_CUDA(cudaMalloc(&vel_, G_ * sizeof(V2<Real>)));
         ICEMPM_CUDA(cudaMalloc(&cur_, G_ * sizeof(V2<Real>)));
         ICEMPM_CUDA(cudaMalloc(&frc_, G_ * sizeof(V4<Real>)));
         ICEMPM_CUDA(cudaMalloc(&status_, G_));
         ICEMPM_CUDA(cudaMalloc(&force_, G_ * sizeof(double2)));
         ICEMPM_CUDA(cudaMalloc(&st_, sizeof(DevStatus)));
-        ICEMPM_CUDA(cudaMemsetAsync(acc_, 0, 3 * G_ * sizeof(Acc), stream_));
+        ICEMPM_CUDA(cudaMemsetAsync(acc_, 0, 3 * Gp_ * sizeof(Acc), stream_));
         ICEMPM_CUDA(cudaMemsetAsync(vel_, 0, G_ * sizeof(V2<Real>), stream_));
         ICEMPM_CUDA(cudaMemsetAsync(force_, 0, G_ * sizeof(double2), stream_));
         ICEMPM_CUDA(cudaMemsetAsync(st_, 0, sizeof(DevStatus), stream_));
@@ -165,7 +166,22 @@ public:
         k.mat = mat_of<Real>(m);
         k.harvest = harvest_;
         k.harvest_stride = harvest_stride_;
+        k.tx_extra = tx_extra_;
+        k.wait_ns = wait_ns_;
         primed_ = false;
+        invalidate_graphs();
+        return 0;
+    }
+
+    // Tests of the barrier-timeout path: each chunk's barrier expects
+    // `extra_bytes` more than its copies deliver, and a wait gives up after
+    // `wait_us` (0, 0 restores the production setting: exact bytes, 1 s).
+    int set_barrier_test(uint32_t extra_bytes, uint32_t wait_us) override
+    {
+        tx_extra_ = extra_bytes;
+        wait_ns_ = wait_us ? 1000ull * wait_us : kWaitLimitNs;
+        kp_.tx_extra = tx_extra_;
+        kp_.wait_ns = wait_ns_;
         invalidate_graphs();
         return 0;
     }
@@ -374,11 +390,12 @@ public:
     // ---------------------------------------------------------------- step
     void launch_update()
     {
-        const unsigned nb = (unsigned)((G_ + 255) / 256);
+        constexpr int NPT = ICEMPM_UPDATE_NPT;
+        const unsigned nb = (unsigned)(((G_ + NPT - 1) / NPT + 255) / 256);
         if (opts_.forcing == ICEMPM_FORCING_EXTENDED)
-            k_grid_update<Real, Acc, true><<<nb, 256, 0, stream_>>>(kp_, grid(), st_, (long long)G_);
+            k_grid_update<Real, Acc, true, NPT><<<nb, 256, 0, stream_>>>(kp_, grid(), st_, (long long)G_);
         else
-            k_grid_update<Real, Acc, false><<<nb, 256, 0, stream_>>>(kp_, grid(), st_, (long long)G_);
+            k_grid_update<Real, Acc, false, NPT><<<nb, 256, 0, stream_>>>(kp_, grid(), st_, (long long)G_);
         launches_++;
     }
 
@@ -396,7 +413,7 @@ public:
     }
     int prime()
     {
-        ICEMPM_CUDA(cudaMemsetAsync(acc_, 0, 3 * G_ * sizeof(Acc), stream_));
+        ICEMPM_CUDA(cudaMemsetAsync(acc_, 0, 3 * Gp_ * sizeof(Acc), stream_));
         ICEMPM_CUDA(cudaMemsetAsync(&st_->err_pending, 0, sizeof(uint32_t), stream_));
         if (n_ > 0) {
             const unsigned nb = (n_ + BT_P2G - 1) / BT_P2G;
@@ -768,7 +785,7 @@ private:
     Grid<Real, Acc> grid() const
     {
         Grid<Real, Acc> g;
-        g.acc.m = acc_; g.acc.px = acc_ + G_; g.acc.py = acc_ + 2 * G_; g.vel = vel_; g.cur = cur_; g.frc = frc_; g.status = status_; g.force = force_;
+        g.acc.m = acc_; g.acc.px = acc_ + Gp_; g.acc.py = acc_ + 2 * Gp_; g.vel = vel_; g.cur = cur_; g.frc = frc_; g.status = status_; g.force = force_;
         return g;
     }
     void invalidate_graphs()
@@ -817,7 +834,8 @@ private:
     void *pts_mem_ = nullptr;
     Pts<Real> pts_[2]{};
     int par_ = 0;
-    Acc *acc_ = nullptr;   // mass, x- and y-momentum arrays of G_ each
+    Acc *acc_ = nullptr;   // mass, x- and y-momentum arrays of G_ each, Gp_ apart
+    size_t Gp_ = 0;
     V2<Real> *vel_ = nullptr, *cur_ = nullptr;
     V4<Real> *frc_ = nullptr;
     double *flow_ab_ = nullptr;   // current frames a, b (2 G_ doubles each), null: static current
@@ -839,6 +857,8 @@ private:
     size_t sort_tmp_bytes_ = 0;
     TileKey tile_{8, 8, 1};
     KParams<Real> kp_{};
+    uint32_t tx_extra_ = 0;
+    unsigned long long wait_ns_ = kWaitLimitNs;
     bool primed_ = false, timed_ = false;
     int fused_ctas_ = 1;
     int steps_since_sort_ = 0;

@@ -42,6 +42,7 @@ public:
     virtual int set_wind_frames(const float *w, int rows, int cols, double cell, double x0, double y0) = 0;
     virtual int set_forcing_time(double tc, double tw) = 0;
     virtual int get_forcing(double *cur, double *stress) = 0;
+    virtual int set_barrier_test(uint32_t extra_bytes, uint32_t wait_us) = 0;
 };
 
 // Ensemble of contexts of one variant stepped together (batch.cuh).

@@ -31,28 +31,30 @@ constexpr int kMaxDevices = 64;
 
 // Static scratch: [keys | alternate keys | alternate values | radix sort temp].  Host
 // code must not use this name as an address: it is a host-side stand-in; the
-// device address comes from cudaGetSymbolAddress at set-up.
+// device address comes from cudaGetSymbolAddress, with the device current.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
 namespace {
 
 std::mutex g_setup_mutex;
-unsigned char *g_scratch_ptr[kMaxDevices] = {};
+bool g_temp_checked[kMaxDevices] = {};
 
-// Once per device, with that device current: resolve the scratch address and
-// check that the radix sort fits its reserved temporary storage.
+// With the device current: the scratch array's device address (looked up on
+// every call, which allocates nothing; a cached address would go stale after
+// cudaDeviceReset), and once per device the check that the radix sort fits
+// its reserved temporary storage.
 int scratch_for_current_device(unsigned char **out)
 {
     int dev = -1;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return icempm::fail(ICEMPM_E_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
     if (dev < 0 || dev >= kMaxDevices) return icempm::fail(ICEMPM_E_UNSUPPORTED, "device ordinal out of range");
+    void *p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess)
+        return icempm::fail(ICEMPM_E_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
     std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_ptr[dev]) {
-        void *p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess)
-            return icempm::fail(ICEMPM_E_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    if (!g_temp_checked[dev]) {
         size_t need = 0;
         cub::DoubleBuffer<uint64_t> kb(nullptr, nullptr);
         cub::DoubleBuffer<uint32_t> vb(nullptr, nullptr);
@@ -63,35 +65,44 @@ int scratch_for_current_device(unsigned char **out)
             return icempm::fail(ICEMPM_E_UNSUPPORTED, "radix sort needs " + std::to_string(need) +
                                                           " bytes of temporary storage, more than the " +
                                                           std::to_string(kTempBytes) + " reserved");
-        g_scratch_ptr[dev] = static_cast<unsigned char *>(p);
+        g_temp_checked[dev] = true;
     }
-    *out = g_scratch_ptr[dev];
+    *out = static_cast<unsigned char *>(p);
     return ICEMPM_OK;
 }
 
-// Key = cell index x*GridY + y in the high word and the point index in the
-// low word (ties in index order); disabled points get the largest key.
+// Bits that hold every value below v (at least 1).
+int bits_below(uint64_t v)
+{
+    int b = 1;
+    while (b < 64 && (v >> b) != 0) b++;
+    return b;
+}
+
+// Key = cell index x*GridY + y shifted above the point index (ties in index
+// order): (cell << ib) | i, below `sentinel` = 1 << (ib + cb); disabled points
+// get the sentinel.  Only the low ib + cb + 1 bits take part in the sort.
 __global__ void k_noalloc_keys(const uint32_t *__restrict__ cell, const uint32_t *__restrict__ util, uint32_t n,
-                               uint32_t gy, uint64_t *keys, uint32_t *vals)
+                               uint32_t gy, int ib, uint64_t sentinel, uint64_t *keys, uint32_t *vals)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    uint64_t key = ~0ull;
+    uint64_t key = sentinel;
     if (!(util[i] & ICEMPM_STATUS_DISABLED)) {
         const uint64_t c = cell[i];
-        key = (((c & 0xffffu) * (uint64_t)gy + (c >> 16)) << 32) | i;
+        key = (((c & 0xffffu) * (uint64_t)gy + (c >> 16)) << ib) | i;
     }
     keys[i] = key;
     vals[i] = i;
 }
 
-// Number of enabled points = length of the leading run of keys below ~0.
-__global__ void k_noalloc_count(const uint64_t *__restrict__ keys, uint32_t n, uint32_t *count)
+// Number of enabled points = length of the leading run of keys below the sentinel.
+__global__ void k_noalloc_count(const uint64_t *__restrict__ keys, uint32_t n, uint64_t sentinel, uint32_t *count)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const bool act = keys[i] != ~0ull;
-    const bool next_inact = (i == n - 1) || keys[i + 1] == ~0ull;
+    const bool act = keys[i] != sentinel;
+    const bool next_inact = (i == n - 1) || keys[i + 1] == sentinel;
     if (act && next_inact) *count = i + 1;
     if (i == 0 && !act) *count = 0;
 }
@@ -122,21 +133,26 @@ extern "C" int icempm_cell_order_noalloc(const uint32_t *d_cell, const uint32_t 
     uint32_t *vals_b = reinterpret_cast<uint32_t *>(scratch + 2 * kKeyBytes);
     void *temp = scratch + 2 * kKeyBytes + kValBytes;
     const unsigned nb = (n + 255) / 256;
+    // cell indices stay below 65536 * grid_y (x and y are 16-bit fields)
+    const int ib = bits_below((uint64_t)n - 1);
+    const int cb = bits_below((uint64_t)65535 * (uint64_t)grid_y + 65535);
+    const int end_bit = ib + cb + 1;
+    const uint64_t sentinel = 1ull << (ib + cb);
     // keys and indices are generated into keys_a and the caller's d_order; the
     // double-buffered radix sort ping-pongs with keys_b / vals_b
-    k_noalloc_keys<<<nb, 256, 0, s>>>(d_cell, d_utility, n, (uint32_t)grid_y, keys_a, d_order);
+    k_noalloc_keys<<<nb, 256, 0, s>>>(d_cell, d_utility, n, (uint32_t)grid_y, ib, sentinel, keys_a, d_order);
     e = cudaGetLastError();
     if (e != cudaSuccess) return icempm::fail(ICEMPM_E_CUDA, std::string("key kernel: ") + cudaGetErrorString(e));
     cub::DoubleBuffer<uint64_t> kb(keys_a, keys_b);
     cub::DoubleBuffer<uint32_t> vb(d_order, vals_b);
     size_t temp_bytes = kTempBytes;
-    e = cub::DeviceRadixSort::SortPairs(temp, temp_bytes, kb, vb, (int)n, 0, 64, s);
+    e = cub::DeviceRadixSort::SortPairs(temp, temp_bytes, kb, vb, (int)n, 0, end_bit, s);
     if (e != cudaSuccess) return icempm::fail(ICEMPM_E_CUDA, std::string("radix sort: ") + cudaGetErrorString(e));
     if (vb.Current() != d_order) {
         e = cudaMemcpyAsync(d_order, vb.Current(), (size_t)n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s);
         if (e != cudaSuccess) return icempm::fail(ICEMPM_E_CUDA, std::string("order copy: ") + cudaGetErrorString(e));
     }
-    k_noalloc_count<<<nb, 256, 0, s>>>(kb.Current(), n, d_count);
+    k_noalloc_count<<<nb, 256, 0, s>>>(kb.Current(), n, sentinel, d_count);
     e = cudaGetLastError();
     if (e != cudaSuccess) return icempm::fail(ICEMPM_E_CUDA, std::string("count kernel: ") + cudaGetErrorString(e));
     return ICEMPM_OK;

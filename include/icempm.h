@@ -312,6 +312,16 @@ ICEMPM_API int icempm_get_stream(icempm_t *ctx, void **stream);
 /* Number of kernel launches this context has enqueued since creation. */
 ICEMPM_API int icempm_launch_count(icempm_t *ctx, uint64_t *count);
 
+/* Test hook of the bounded device waits (no counterpart in the reference,
+ * whose kernels do not wait on copies).  The fused kernel waits on a barrier
+ * for each chunk's point state; with extra_bytes > 0 every such barrier
+ * expects extra_bytes more than the copies deliver, so the wait runs out
+ * after wait_limit_us although every copy has landed, and the step raises
+ * ICEMPM_ERR_BARRIER_TIMEOUT instead of hanging.  (0, 0) restores the
+ * production setting (exact byte counts, 1 s limit).  The context stays
+ * usable: icempm_update_constants clears the error word. */
+ICEMPM_API int icempm_debug_barrier_timeout(icempm_t *ctx, uint32_t extra_bytes, uint32_t wait_limit_us);
+
 /* Largest point count icempm_cell_order_noalloc accepts. */
 #define ICEMPM_NOALLOC_MAX_POINTS (1u << 20)
 
@@ -364,8 +374,9 @@ ICEMPM_API int icempm_prepare_frame(icempm_t *ctx, const uint32_t *point_colors_
 typedef struct icempm_batch icempm_batch_t;
 
 typedef struct icempm_batch_tuning_t {
-    int32_t tile_nodes;    /* shared scatter tile of the fused kernel: 512 or 1024 nodes */
-    int32_t stages;        /* bulk-copy stages of point state: 1 or 2 (512 nodes only) */
+    int32_t tile_nodes;    /* shared scatter tile of the fused kernel: 0 (none: node sums go
+                              straight to the global accumulators), 512 or 1024 nodes */
+    int32_t stages;        /* bulk-copy stages of point state: 1 or 2 (2 without a tile only) */
     int32_t sort_every;    /* locality sort of every scene each this many sub-steps; 0 = never */
     int32_t graph_steps;   /* sub-steps per CUDA graph; 0 = direct launches */
     float ms_per_step;     /* set by icempm_batch_autotune: the chosen form's time per sub-step */

@@ -97,3 +97,10 @@ def test_device_count_is_safe_without_gpu(lib):
     n = C.c_int(-5)
     lib.icempm_device_count(C.byref(n))
     assert n.value >= 0
+
+
+def test_noalloc_rejects_oversize_before_any_device_work(lib):
+    """icempm_cell_order_noalloc refuses n above ICEMPM_NOALLOC_MAX_POINTS with
+    ICEMPM_E_CAPACITY and a message, before it touches a device (no GPU here)."""
+    rc = lib.icempm_cell_order_noalloc(None, None, (1 << 20) + 1, 8, None, None, None)
+    assert rc == -5 and b"ICEMPM_NOALLOC_MAX_POINTS" in lib.icempm_last_error()

@@ -89,7 +89,7 @@ def test_autotune_picks_a_supported_form_and_stepping_goes_on(capi, small_ensemb
     ctxs = open_contexts(capi, scs)
     with capi.Batch(ctxs) as b:
         t = b.autotune(trial_steps=50, first_step=0)
-        assert (t.tile_nodes, t.stages) in [(512, 1), (1024, 1), (512, 2)]
+        assert (t.tile_nodes, t.stages) in [(0, 2), (0, 1), (512, 1), (1024, 1)]
         assert t.sort_every in (0, 100, 400) and t.graph_steps == 50 and t.ms_per_step > 0
         b.step(60, 200)
     for c, sc in zip(ctxs, scs):

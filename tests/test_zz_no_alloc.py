@@ -72,8 +72,40 @@ def test_noalloc_order_matches_sort_compact_twice():
         assert np.array_equal(got.view(np.uint64), ref[:, :m].view(np.uint64))
 
 
-def test_noalloc_rejects_oversize_without_touching_memory():
+def _pts(seed, n, disabled_frac, gx=48, gy=40):
+    """n points on random cells of a gx x gy grid (several per cell), a
+    fraction of them disabled; only the cell and utility rows matter here."""
+    rng = np.random.default_rng(seed)
+    soa = np.zeros((19, max(n, 1)))
+    cx = rng.integers(2, gx - 2, n).astype(np.uint32)
+    cy = rng.integers(2, gy - 2, n).astype(np.uint32)
+    H.set_u32(soa, IDX_CELL, (cy << 16) | cx, n)
+    util = np.where(rng.random(n) < disabled_frac, STATUS_DISABLED, 0).astype(np.uint32)
+    H.set_u32(soa, IDX_UTILITY, util, n)
+    return soa
+
+
+def expected_order(soa, n, grid_y):
+    """The compaction order by definition: enabled points, stable by cell index x*grid_y + y."""
+    cell = H.get_u32(soa, IDX_CELL, n).astype(np.int64)
+    util = H.get_u32(soa, IDX_UTILITY, n)
+    idx = np.nonzero((util & STATUS_DISABLED) == 0)[0]
+    key = (cell[idx] & 0xffff) * grid_y + (cell[idx] >> 16)
+    return idx[np.argsort(key, kind="stable")].astype(np.uint32)
+
+
+@pytest.mark.parametrize("n,disabled_frac", [(0, 0.0), (100, 0.3), (257, 1.0), (5000, 0.1)])
+def test_noalloc_edge_sizes_twice(n, disabled_frac):
+    """No points, a small set (the sort's single-tile path), every point
+    disabled, and a few thousand points: the count and the order, bit for bit,
+    on two calls in a row."""
     from icempm_2d_sp_b200 import capi
-    L = capi.load()
-    rc = L.icempm_cell_order_noalloc(None, None, (1 << 20) + 1, 8, None, None, None)
-    assert rc == -5 and b"ICEMPM_NOALLOC_MAX_POINTS" in L.icempm_last_error()
+    capi.load()
+    if capi.device_count() < 1:
+        pytest.fail("no CUDA device visible to the library")
+    soa = _pts(7 + n, n, disabled_frac)
+    want = expected_order(soa, n, 40)
+    for _ in range(2):
+        order, count = order_noalloc(capi, soa, n, 40)
+        assert count == len(want)
+        assert np.array_equal(order[:count], want)

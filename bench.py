@@ -51,9 +51,16 @@ B_POINT, B_NODE = 124, 49
 # split of the node bytes: the fused G2P+P2G kernel reads 8 B of velocity and
 # flushes 12 B of accumulators per node; the grid update moves the other 29 B
 B_NODE_FUSED = 20
-# measured DRAM traffic of the fused kernel per point, grid share included
-# (489.86 MB for 5,884,928 points and 2,097,152 nodes in one launch)
-TRAFFIC_B_PER_POINT = 83.24
+# DRAM traffic of one fused-kernel launch per point, grid share included:
+# dram__bytes_read.sum + dram__bytes_write.sum of an ncu capture of one
+# k_g2p_p2g launch on the floe field at 2048x1024 (the summary in
+# profiles/k_g2p_p2g_floe_field_2048x1024.md), scaled by point count (the
+# node/point ratio is the same at 4096x2048)
+TRAFFIC_B_PER_POINT = 82.84
+TRAFFIC_CAPTURE = {"capture": "profiles/k_g2p_p2g_floe_field_2048x1024.md", "points": 5884928,
+                   "dram_bytes": 487512320, "scaled_by": "points"}
+# the ~8.4M-point variant of the scene reported beside the main line
+POINTS_8M = 8_400_000
 
 
 def parse():
@@ -72,6 +79,8 @@ def parse():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=4)
     ap.add_argument("--no-ref-gpu", action="store_true")
+    ap.add_argument("--no-8m", action="store_true",
+                    help="skip the ~8.4M-point variant timed beside the main line (chosen, fp32, reference CUDA step)")
     ap.add_argument("--ref-gpu-steps", type=int, default=50)
     ap.add_argument("--grid", type=int, nargs=2, default=None, metavar=("GX", "GY"),
                     help="same scene rules on a smaller GX x GY grid (seeds scaled by area), "
@@ -349,7 +358,7 @@ def main():
 
     import torch
     from icempm_2d_sp_b200 import capi
-    from icempm_2d_sp_b200.params import Options, VARIANT_FIXED, VARIANT_FP32
+    from icempm_2d_sp_b200.params import Options, VARIANT_FIXED, VARIANT_FP32, VARIANT_TEXTBOOK
 
     def sync_all():
         torch.cuda.synchronize()
@@ -360,7 +369,8 @@ def main():
     n, G = sc.n, sc.grid_nodes
     peak, peak_src = load_peaks()
 
-    def timed(variant):
+    def timed(variant, sc=sc):
+        n = sc.n
         o = Options.default(forcing=sc.options.forcing)
         for f, _ in Options._fields_:
             setattr(o, f, getattr(sc.options, f))
@@ -388,11 +398,20 @@ def main():
     t_ms, n_tot = combine_ranks(dist, total, n)
     value = n_tot * args.steps / (t_ms * 1e-3)
 
-    plain = None
+    # the plain from-scratch FP32 step (three unfused kernels, one point per
+    # thread, global FP32 atomics) and the fused engine with FP32 atomics
+    plain = fp32_atomics = None
     if not args.no_plain:
+        ttot, tupd, tpts, _, _, terr = timed(VARIANT_TEXTBOOK)
+        plain = {"value": n * args.steps / (ttot * 1e-3), "ms_per_step": ttot / args.steps,
+                 "points_kernels_ms": tpts / args.steps, "grid_update_ms": tupd / args.steps, "device_errors": terr,
+                 "variant": "textbook: P2G with 27 global FP32 atomics per point, grid update, G2P; "
+                            "one point per thread, unfused (ICEMPM_VARIANT_TEXTBOOK)",
+                 "chosen_speedup": ttot / total}
         ptot, pupd, pfused, _, _, _ = timed(VARIANT_FP32)
-        plain = {"value": n * args.steps / (ptot * 1e-3), "ms_per_step": ptot / args.steps,
-                 "fused_kernel_ms": pfused / args.steps, "variant": "fp32 atomics (plain)"}
+        fp32_atomics = {"value": n * args.steps / (ptot * 1e-3), "ms_per_step": ptot / args.steps,
+                        "fused_kernel_ms": pfused / args.steps,
+                        "variant": "the fused engine with FP32 atomics instead of fixed point"}
 
     # roofline of the dominant kernel (fused G2P+P2G), live events of the timed region
     fused_bytes = B_POINT * n + B_NODE_FUSED * G
@@ -404,6 +423,9 @@ def main():
     traffic = TRAFFIC_B_PER_POINT * n
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": traffic, "peak_source": peak_src,
+                "traffic_source": dict(TRAFFIC_CAPTURE, bytes_per_point=TRAFFIC_B_PER_POINT,
+                                       note="measured on the capture, scaled to this launch; not measured live"),
+                "dram_frac": traffic / fused_launch_s / 1e9 / peak,
                 "kernel": "k_g2p_p2g (fused G2P + P2G)", "algorithmic_bytes_per_launch": fused_bytes,
                 "avg_launch_ms": fused * 1e-3 / args.steps * 1e3,
                 "step_bytes": B_POINT * n + B_NODE * G,
@@ -420,6 +442,25 @@ def main():
     ref_gpu = None
     if rank == 0 and world == 1 and not args.no_ref_gpu:
         ref_gpu = reference_gpu_baseline(args, sc)
+    # the ~8.4M-point variant (whole floes of the same scene kept until 8.4M
+    # points): chosen form, FP32 atomics and the reference's CUDA step
+    scene_8m = None
+    if rank == 0 and world == 1 and not args.no_8m and args.grid is None and args.max_points is None:
+        s8 = make_scene(1235, max_points=POINTS_8M)
+        t8, u8, f8, _, _, e8 = timed(VARIANT_FIXED, s8)
+        p8, _, pf8, _, _, _ = timed(VARIANT_FP32, s8)
+        b8, _, _, _, _, _ = timed(VARIANT_TEXTBOOK, s8)
+        scene_8m = {"points": int(s8.n), "grid_nodes": s8.grid_nodes,
+                    "value": s8.n * args.steps / (t8 * 1e-3), "ms_per_step": t8 / args.steps,
+                    "fused_kernel_ms": f8 / args.steps, "grid_update_ms": u8 / args.steps, "device_errors": e8,
+                    "plain": {"value": s8.n * args.steps / (b8 * 1e-3), "ms_per_step": b8 / args.steps,
+                              "variant": "textbook (see plain)", "chosen_speedup": b8 / t8},
+                    "fp32_atomics": {"value": s8.n * args.steps / (p8 * 1e-3), "ms_per_step": p8 / args.steps}}
+        if not args.no_ref_gpu:
+            r8 = reference_gpu_baseline(args, s8)
+            scene_8m["reference_gpu"] = r8
+            if "ms_per_step" in r8:
+                scene_8m["speedup_vs_reference_gpu"] = r8["ms_per_step"] / (t8 / args.steps)
 
     if rank == 0:
         workload = WORKLOAD if args.grid is None else WORKLOAD.replace("4096x2048", "%dx%d" % tuple(args.grid))
@@ -433,7 +474,9 @@ def main():
                            "parallelism": f"{world} independent scene(s), one per GPU",
                            "l2": "inputs larger than L2 (2.0 GB point state, 0.4 GB grid)",
                            "device_errors": err},
-                "plain": plain, "reference_gpu": ref_gpu, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+                "plain": plain, "fp32_atomics": fp32_atomics, "reference_gpu": ref_gpu, "scene_8m": scene_8m,
+                "roofline": roofline,
+                "cpu_baseline": cpu, "e2e": e2e,
                 "gpu_launches": launches, "clocks": clocks}
         print(json.dumps(line), flush=True)
     if dist:

@@ -26,6 +26,7 @@ EXPORTS = [
     "icempm_return_map_learned", "icempm_harvest_begin", "icempm_harvest_end", "icempm_prepare_frame",
     "icempm_set_flow_frames", "icempm_set_wind_frames", "icempm_set_forcing_time", "icempm_get_forcing",
     "icempm_download_points_async", "icempm_download_wait", "icempm_debug_barrier_timeout",
+    "icempm_set_learned_map", "icempm_learned_map_counts", "icempm_tune_sort_cadence",
 ]
 
 FRAME_CHANNELS = ("point_density", "mass", "vx", "vy", "Jpinv", "P", "Q", "r", "g", "b")
@@ -85,6 +86,9 @@ def load(path: str = LIB_PATH):
         "icempm_download_points_async": (C.c_int, [h, dp, C.c_uint32, C.POINTER(C.c_uint32)]),
         "icempm_download_wait": (C.c_int, [h]),
         "icempm_debug_barrier_timeout": (C.c_int, [h, C.c_uint32, C.c_uint32]),
+        "icempm_set_learned_map": (C.c_int, [h, C.c_void_p, C.c_void_p, C.c_float]),
+        "icempm_tune_sort_cadence": (C.c_int, [h, C.c_int32, C.c_int32, C.POINTER(C.c_int32)]),
+        "icempm_learned_map_counts": (C.c_int, [h, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
         "icempm_get_status": (C.c_int, [h, C.POINTER(C.c_uint32), C.POINTER(C.c_int32)]),
         "icempm_clear_force_accumulator": (C.c_int, [h]),
         "icempm_get_boundary_forces": (C.c_int, [h, dp, C.c_int32]),
@@ -292,6 +296,24 @@ class Context:
     def download_wait(self):
         check(self._L.icempm_download_wait(self.h))
         self._pending = None
+
+    def tune_sort_cadence(self, trial_steps: int, first_step: int = 0) -> int:
+        """Measure and set the locality re-sort cadence (advances the scene
+        2 * trial_steps sub-steps); returns it (0: no periodic sort)."""
+        k = C.c_int32(0)
+        check(self._L.icempm_tune_sort_cadence(self.h, int(trial_steps), int(first_step), C.byref(k)))
+        return k.value
+
+    def set_learned_map(self, params_ptr, norm_ptr, tol: float):
+        """Put the learned return map on the step path (device pointers to the
+        FP32 parameters and the 14-float normalisation; params_ptr None: off)."""
+        check(self._L.icempm_set_learned_map(self.h, params_ptr, norm_ptr, float(tol)))
+
+    def learned_map_counts(self) -> tuple:
+        """(answers kept, exact fallbacks) of the learned map since it was set."""
+        a, b = C.c_uint64(0), C.c_uint64(0)
+        check(self._L.icempm_learned_map_counts(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
 
     def debug_barrier_timeout(self, extra_bytes: int, wait_limit_us: int):
         """Test hook: make the fused kernel's chunk barriers expect extra_bytes

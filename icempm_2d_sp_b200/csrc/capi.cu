@@ -84,6 +84,7 @@ int icempm_create(const icempm_simparams_t *prms, const uint8_t *grid_status, co
     case ICEMPM_VARIANT_FIXED: e = icempm::make_engine_fixed(); break;
     case ICEMPM_VARIANT_FP32: e = icempm::make_engine_fp32(); break;
     case ICEMPM_VARIANT_FP64: e = icempm::make_engine_fp64(); break;
+    case ICEMPM_VARIANT_TEXTBOOK: e = icempm::make_engine_fp32(); break;   // FP32 engine, textbook step
     default: return fail(ICEMPM_E_ARG, "unknown variant");
     }
     icempm_context *c = new (std::nothrow) icempm_context;
@@ -300,6 +301,24 @@ int icempm_harvest_end(icempm_t *ctx, float *records, uint32_t capacity, uint32_
     ICEMPM_TRY(ctx->eng->harvest_end(records, capacity, count));
 }
 
+int icempm_set_learned_map(icempm_t *ctx, const float *d_params, const float *d_norm, float tol)
+{
+    ICEMPM_GUARD_CTX(ctx);
+    ICEMPM_TRY(ctx->eng->set_learned_map(d_params, d_norm, tol));
+}
+
+int icempm_learned_map_counts(icempm_t *ctx, uint64_t *kept, uint64_t *fallbacks)
+{
+    ICEMPM_GUARD_CTX(ctx);
+    ICEMPM_TRY(ctx->eng->learned_counts(kept, fallbacks));
+}
+
+int icempm_tune_sort_cadence(icempm_t *ctx, int32_t trial_steps, int32_t first_step, int32_t *sort_every)
+{
+    ICEMPM_GUARD_CTX(ctx);
+    ICEMPM_TRY(ctx->eng->tune_sort(trial_steps, first_step, sort_every));
+}
+
 int icempm_debug_barrier_timeout(icempm_t *ctx, uint32_t extra_bytes, uint32_t wait_limit_us)
 {
     if (extra_bytes % 16u != 0) return fail(ICEMPM_E_ARG, "extra_bytes must be a multiple of 16");
@@ -325,7 +344,7 @@ int icempm_batch_create(icempm_t *const *contexts, int32_t count, icempm_batch_t
         case ICEMPM_VARIANT_FIXED: b = icempm::make_batch_fixed(eng.data(), count); break;
         case ICEMPM_VARIANT_FP32: b = icempm::make_batch_fp32(eng.data(), count); break;
         case ICEMPM_VARIANT_FP64: b = icempm::make_batch_fp64(eng.data(), count); break;
-        default: return fail(ICEMPM_E_ARG, "unknown variant");
+        default: return fail(ICEMPM_E_ARG, "batches take the fixed, fp32 or fp64 variant");
         }
     } catch (const std::bad_alloc &) {
         return fail(ICEMPM_E_NOMEM, "host allocation failed");

@@ -43,6 +43,7 @@
 
 #include "device_math.cuh"
 #include "icempm.h"
+#include "mlp_device.cuh"
 
 // Shape of the FP32-state fused kernel: threads per CTA, points per thread,
 // nodes of the shared scatter tile (0: no tile, each warp's merged node sums
@@ -193,6 +194,9 @@ template <class Real> struct KParams {
     int harvest_stride;             // ... for points with (index + step) % stride == 0
     uint32_t tx_extra;              // bytes each chunk's barrier expects beyond its copies (0; tests of the timeout)
     unsigned long long wait_ns;     // time limit of a barrier wait
+    const mlp::Packed *mlp;         // learned return map (the LEARNED instance): packed network
+    float mlp_tol;                  // ... accepted when its answer lies on the yield surface within this
+    unsigned long long *mlp_counts; // ... [0] answers kept, [1] exact fallbacks
 };
 
 // Fire-and-forget reductions into global memory (red.global: no value comes
@@ -477,6 +481,141 @@ __global__ void __launch_bounds__(BT) k_p2g(KParams<Real> kp, Pts<Real> P, Grid<
     __syncthreads();
     tile_flush<Acc, CAP, BT>(T, G.acc, kp.gx, kp.gy);
     warp_flush_status(st, 0u, perr, 0);
+}
+
+// ---- the textbook step: the plain from-scratch FP32 baseline ---------------
+// The MPM sub-step as three plain kernels, one point or node per thread,
+// written the way the method is usually first put on a GPU: P2G straight into
+// the global accumulators with one FP32 atomic per node and channel (27 per
+// point), the grid update, and G2P with the 3x3 gather summed node by node;
+// the whole point state (V and C included) is read and written every
+// sub-step.  Same arithmetic helpers as the fused kernel (H = Fe - I, FP32),
+// no fusion, no locality tiles, no warp-level merging, no fixed point.  It is
+// the yardstick the fused kernel is measured against, not the product.
+// P2G of the next sub-step (errors pending until its grid update, as in the
+// fused kernel); `advance`: the sub-step counter moves on (not when priming).
+template <class Real>
+__global__ void __launch_bounds__(256) k_textbook_p2g(KParams<Real> kp, Pts<Real> P, Grid<Real, float> G,
+                                                      DevStatus *st, int n, int advance)
+{
+    const int i = blockIdx.x * 256 + threadIdx.x;
+    if (advance && i == 0) st->step += 1;   // G2P of this sub-step has finished reading it
+    uint32_t perr = 0;
+    if (i < n) {
+        const uint2 key = P.K[i];
+        if (!(key.y & kDisabled)) {
+            Src<Real> s;
+            s.cx = (int)(key.x & 0xffff); s.cy = (int)(key.x >> 16);
+            if (cell_in_range(s.cx, s.cy, kp.gx, kp.gy)) {
+                const V4<Real> A = P.A[i], Hv = P.H[i], Cv = P.C[i];
+                const V2<Real> v = P.V[i];
+                const M2<Real> H = {Hv.x, Hv.y, Hv.z, Hv.w};
+                V4<Real> f{};
+                if (kp.ext) f = G.frc[(uint32_t)s.cx * (uint32_t)kp.gy + (uint32_t)s.cy];
+                make_src<Real, float>(kp, f, s, A.x, A.y, A.z, A.w, kinematics(H), v.x, v.y, Cv.x, Cv.y, Cv.z, Cv.w,
+                                      perr);
+                bool nan_m = false, nan_v = false;
+                for (int a = 0; a < 3; a++)
+                    for (int b = 0; b < 3; b++) {
+                        Real m, px, py;
+                        src_terms(s, a, b, m, px, py);
+                        nan_m |= isnan(m);
+                        nan_v |= isnan(px) || isnan(py);
+                        const uint32_t node = (uint32_t)(s.cx + a - 1) * (uint32_t)kp.gy + (uint32_t)(s.cy + b - 1);
+                        atomicAdd(G.acc.m + node, float(m));
+                        atomicAdd(G.acc.px + node, float(px));
+                        atomicAdd(G.acc.py + node, float(py));
+                    }
+                if (nan_m) perr |= kErrP2gNanMass;
+                if (nan_v) perr |= kErrP2gNanVel;
+            } else {
+                perr |= kErrLeftArea;
+            }
+        }
+    }
+    warp_flush_status(st, 0u, perr, 0);
+}
+
+template <class Real>
+__global__ void __launch_bounds__(256) k_textbook_g2p(KParams<Real> kp, Pts<Real> P, Grid<Real, float> G,
+                                                      DevStatus *st, int n)
+{
+    const int i = blockIdx.x * 256 + threadIdx.x;
+    uint32_t err = 0;
+    int ndis = 0;
+    const int step = st->step;
+    if (i < n) {
+        const uint2 key = P.K[i];
+        uint32_t util = key.y;
+        if (!(util & kDisabled)) {
+            const V4<Real> A = P.A[i], Hv = P.H[i];
+            Real x = A.x, y = A.y, Jp = A.z;
+            const Real thick = A.w;
+            M2<Real> H = {Hv.x, Hv.y, Hv.z, Hv.w};
+            int cx = (int)(key.x & 0xffff), cy = (int)(key.x >> 16);
+            Real vx = 0, vy = 0, c00 = 0, c01 = 0, c10 = 0, c11 = 0;
+            if (cell_in_range(cx, cy, kp.gx, kp.gy)) {
+                Real wx[3], wy[3];
+                bspline(x, wx);
+                bspline(y, wy);
+                for (int a = 0; a < 3; a++)
+                    for (int b = 0; b < 3; b++) {
+                        const V2<Real> nv = G.vel[(uint32_t)(cx + a - 1) * (uint32_t)kp.gy + (uint32_t)(cy + b - 1)];
+                        const Real w = wx[a] * wy[b];
+                        const Real dx = Real(a - 1) - x, dy = Real(b - 1) - y;
+                        vx += w * nv.x; vy += w * nv.y;
+                        c00 += w * nv.x * dx; c01 += w * nv.x * dy;
+                        c10 += w * nv.y * dx; c11 += w * nv.y * dy;
+                    }
+                c00 *= kp.four_h_inv; c01 *= kp.four_h_inv; c10 *= kp.four_h_inv; c11 *= kp.four_h_inv;
+            }
+            x += vx * kp.dt_h_inv;
+            y += vy * kp.dt_h_inv;
+            if (isnan(vx + vy)) err |= kErrVelNan;
+            if (isnan(x + y)) err |= kErrPosNan;
+            if (isnan((c00 + c10) + (c01 + c11))) err |= kErrBpNan;
+            bool moved = false;
+            if (x > Real(0.5)) { x -= Real(1); cx++; moved = true; }
+            else if (x < Real(-0.5)) { x += Real(1); cx--; moved = true; }
+            if (y > Real(0.5)) { y -= Real(1); cy++; moved = true; }
+            else if (y < Real(-0.5)) { y += Real(1); cy--; moved = true; }
+            if (moved && (cx <= 1 || cx >= kp.gx - 2 || cy <= 1 || cy >= kp.gy - 2)) {
+                util |= kDisabled;
+                ndis++;
+            }
+            if (x > Real(0.5) || x < Real(-0.5) || y > Real(0.5) || y < Real(-0.5)) err |= kErrJump;
+            const Real d00 = kp.dt * c00, d01 = kp.dt * c01, d10 = kp.dt * c10, d11 = kp.dt * c11;
+            const M2<Real> h = H;
+            H.a00 = h.a00 + d00 + (d00 * h.a00 + d01 * h.a10);
+            H.a01 = h.a01 + d01 + (d00 * h.a01 + d01 * h.a11);
+            H.a10 = h.a10 + d10 + (d10 * h.a00 + d11 * h.a10);
+            H.a11 = h.a11 + d11 + (d10 * h.a01 + d11 * h.a11);
+            if (isnan((H.a00 + H.a10) + (H.a01 + H.a11))) err |= kErrFeNan;
+            Kin<Real> k = kinematics(H);
+            Real p_tr, q_tr;
+            pq(k, kp.mat.mu, kp.mat.kappa, p_tr, q_tr);
+            if (!(util & kCrushed)) util = failure_check(kp.mat, util, p_tr, q_tr);
+            if (util & kCrushed) {
+                wolper_dp(kp.mat, thick, p_tr, q_tr, k, svd_h(H), H, Jp);
+                if (isnan((H.a00 + H.a10) + (H.a01 + H.a11))) err |= kErrFeNan;
+            }
+            V4<Real> Ao; Ao.x = x; Ao.y = y; Ao.z = Jp; Ao.w = thick;
+            P.A[i] = Ao;
+            V4<Real> Ho; Ho.x = H.a00; Ho.y = H.a01; Ho.z = H.a10; Ho.w = H.a11;
+            P.H[i] = Ho;
+            V2<Real> Vo; Vo.x = vx; Vo.y = vy;
+            P.V[i] = Vo;
+            V4<Real> Co; Co.x = c00; Co.y = c01; Co.z = c10; Co.w = c11;
+            P.C[i] = Co;
+            uint2 ko; ko.x = ((uint32_t)cy << 16) | (uint32_t)cx; ko.y = util;
+            P.K[i] = ko;
+            if (kp.update_every > 0 && (step % kp.update_every) == 0) {
+                V2<Real> pqv; pqv.x = p_tr; pqv.y = q_tr;
+                P.PQ[i] = pqv;
+            }
+        }
+    }
+    warp_flush_status(st, err, 0u, ndis);
 }
 
 // ---- grid update (partition_kernel_update_nodes, kernels.cuh:109-177) ----
@@ -867,6 +1006,8 @@ template <class Real, class Acc, int BT, int PPT, int CAP, int STAGES> struct Ch
 
 // Cell word of a stage entry whose point scatters nothing this step.
 constexpr uint32_t kNoScatter = 0xffffffffu;
+// Instances of the fused kernel (template argument MODE).
+constexpr int FUSED_PLAIN = 0, FUSED_HARVEST = 1, FUSED_LEARNED = 2;
 
 // The source's mass: in the K entry's second word (FP32 state, returned as
 // that word) or in the stage's mass array (FP64 state, returns 0).
@@ -928,12 +1069,81 @@ __device__ __noinline__ void harvest_record(HarvestBuf *hb, const MatT<Real> &m,
     hb->rec[2 * (size_t)r + 1] = make_float4(float(Real(1) + s1.e0), float(Real(1) + s1.e1), float(jp1), 3.0f);
 }
 
+// Case 3 of wolper_dp (kernels.cuh:400-467): the trial state lies above the
+// yield surface and is projected onto it.
+template <class T> __device__ __forceinline__ bool is_projection(const MatT<T> &m, T p_tr, T q_tr)
+{
+    if (p_tr < m.thr) return false;
+    T q_yield = T(0);
+    if (p_tr < m.pmax) q_yield = fmin(m.fs_c * tsqrt((m.pmax - p_tr) * (p_tr - m.pmin)), fmax(T(0), (p_tr - m.thr) * m.tan_phi));
+    return q_tr > q_yield;
+}
+
+// The learned return map in place of wolper_dp's case 3, for the lanes with
+// `net` (all 32 lanes of the warp call it; the network runs on the warp's
+// rows).  Inputs (log sigma1, log sigma2, log Jp_inv, log thickness) and
+// outputs (the log changes of sigma1, sigma2, Jp_inv) are standardised with
+// the network's norm.  An answer is kept when it lies on the yield surface
+// within kp.mlp_tol (|q - q_yield(p)| / max(q_yield, 1) of the predicted
+// state); otherwise, and for non-finite answers, the exact map answers.  The
+// rotations U, V of the trial state's SVD are kept.  Counts go to
+// kp.mlp_counts (kept, fallback).
+template <class Real, int NW>
+__device__ __noinline__ void learned_projection(const KParams<Real> &kp, mlp::Smem<NW> &ml, int wid, int lane, bool net,
+                                                Real thick, Real p_tr, Real q_tr, const SvdH<Real> &svd,
+                                                Kin<Real> &k, M2<Real> &H, Real &Jp)
+{
+    const float *nm = ml.p.norm;
+    float xin[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    if (net) {
+        xin[0] = (log1pf(float(svd.e0)) - nm[0]) / nm[4];
+        xin[1] = (log1pf(float(svd.e1)) - nm[1]) / nm[5];
+        xin[2] = (logf(float(Jp)) - nm[2]) / nm[6];
+        xin[3] = (logf(float(thick)) - nm[3]) / nm[7];
+    }
+    float yo[3];
+    mlp::rows_forward(ml.p, ml.io[wid], lane, xin, yo);
+    bool kept = false;
+    if (net) {
+        const MatT<Real> &m = kp.mat;
+        const Real y0 = Real(yo[0] * nm[11] + nm[8]), y1 = Real(yo[1] * nm[12] + nm[9]), y2 = Real(yo[2] * nm[13] + nm[10]);
+        // sigma' - 1 = e + (1 + e)(exp(y) - 1)
+        const Real e0 = svd.e0 + (Real(1) + svd.e0) * Real(expm1f(float(y0)));
+        const Real e1 = svd.e1 + (Real(1) + svd.e1) * Real(expm1f(float(y1)));
+        const Real jp1 = Jp * Real(expf(float(y2)));
+        const Real s0 = Real(1) + e0, s1 = Real(1) + e1;
+        const Real J1 = s0 * s1;
+        const Real p1 = -(m.kappa * Real(0.5)) * (J1 * J1 - Real(1));
+        const Real q1 = m.mu * fabs((e0 - e1) * (Real(2) + e0 + e1)) / J1;   // mu |s0^2 - s1^2| / J
+        Real qy = Real(0);
+        if (p1 < m.pmax)
+            qy = fmin(m.fs_c * tsqrt(fmax((m.pmax - p1) * (p1 - m.pmin), Real(0))), fmax(Real(0), (p1 - m.thr) * m.tan_phi));
+        const Real res = fabs(q1 - qy) / fmax(qy, Real(1));
+        kept = res <= Real(kp.mlp_tol) && isfinite(e0) && isfinite(e1) && isfinite(jp1) && jp1 > Real(0);
+        if (kept) {
+            H = usvt_h(svd, e0, e1);
+            Jp = jp1;
+        } else {
+            wolper_dp(kp.mat, thick, p_tr, q_tr, k, svd, H, Jp);
+        }
+    }
+    const unsigned nk = __popc(__ballot_sync(0xffffffffu, kept));
+    const unsigned nf = __popc(__ballot_sync(0xffffffffu, net && !kept));
+    if (lane == 0) {
+        if (nk) atomicAdd(&kp.mlp_counts[0], (unsigned long long)nk);
+        if (nf) atomicAdd(&kp.mlp_counts[1], (unsigned long long)nf);
+    }
+}
+
 // One chunk of the fused kernel: CH = BT*PPT entries starting at `base` of a
 // scene's arrays, whose A, H, K are in stage `s`.  With one stage, the next
 // chunk (`next`, arrays Pn from base_n) is fetched into it once its points
 // are read.  Error bits and the count of newly disabled points accumulate
-// into err, perr, ndis.  HARVEST: the instance that records return-map pairs
-// (kept out of the ordinary instance, whose registers it would crowd).
+// into err, perr, ndis.  MODE: 0 the ordinary instance, FUSED_HARVEST the one
+// that records return-map pairs, FUSED_LEARNED the one whose projections onto
+// the yield surface go to the learned return map (both kept out of the
+// ordinary instance, whose registers they would crowd); ml is the learned
+// map's shared memory (FUSED_LEARNED only).
 //
 // G2P follows partition_kernel_g2p (kernels.cuh:181-315), P2G
 // partition_kernel_p2g (kernels.cuh:39-104).  Two phases per chunk:
@@ -958,12 +1168,12 @@ __device__ __noinline__ void harvest_record(HarvestBuf *hb, const MatT<Real> &m,
 // cancels because sum_a wx_a (a-1-x) = 0 and sum_b wy_b (b-1-y) = 0) and keeps
 // FP32 roundoff relative to velocity differences.  Velocities, momenta and
 // the columns of C are pairs (packed FP32x2 arithmetic).
-template <class Real, class Acc, int BT, int PPT, int CAP, int STAGES, bool HARVEST>
+template <class Real, class Acc, int BT, int PPT, int CAP, int STAGES, int MODE>
 __device__ __forceinline__ void fused_chunk(ChunkSmem<Real, Acc, BT, PPT, CAP, STAGES> &sm, int s,
                                             const KParams<Real> &kp, const Pts<Real> &P, const Grid<Real, Acc> &G,
                                             uint32_t base, int n, int step, bool recordPQ, bool store_vc, bool next,
                                             const Pts<Real> &Pn, uint32_t base_n, uint32_t &err, uint32_t &perr,
-                                            int &ndis)
+                                            int &ndis, mlp::Smem<BT / 32> *ml = nullptr)
 {
     using SM = ChunkSmem<Real, Acc, BT, PPT, CAP, STAGES>;
     using PT = P2<Real>;
@@ -985,183 +1195,213 @@ __device__ __forceinline__ void fused_chunk(ChunkSmem<Real, Acc, BT, PPT, CAP, S
     for (int j = 0; j < PPT; j++) {
         const int local = wbase + 32 * j;
         const uint32_t i = base + (uint32_t)local;
-        if (i >= (uint32_t)n) break;
-        const uint2 key = sg.K[local];
+        const bool inb = i < (uint32_t)n;
+        const uint2 key = inb ? sg.K[local] : make_uint2(0u, kDisabled);
         uint32_t util = key.y;
-        if (util & kDisabled) { sg.K[local].x = kNoScatter; continue; }
-        const V4<Real> A = sg.A[local];
-        const V4<Real> Hv = sg.H[local];
-        Real Jp = A.z;
-        const Real thick = A.w;
-        M2<Real> H = {Hv.x, Hv.y, Hv.z, Hv.w};
-        int cx = (int)(key.x & 0xffff), cy = (int)(key.x >> 16);
-        PT v = pbc(Real(0)), c0 = pbc(Real(0)), c1 = pbc(Real(0));   // (vx, vy), (c00, c10), (c01, c11)
-        if (cell_in_range(cx, cy, kp.gx, kp.gy)) {
-            if (!ICEMPM_VEL_CACHE || key.x != vcell) {
-                vcell = key.x;
-                const V2<Real> *col = G.vel + ((uint32_t)(cx - 1) * (uint32_t)kp.gy + (uint32_t)(cy - 1));
-                PT nv[3][3];
-#pragma unroll
-                for (int a = 0; a < 3; a++)
-#pragma unroll
-                    for (int b = 0; b < 3; b++) nv[a][b] = ld_vel(col + (uint32_t)a * (uint32_t)kp.gy + b);
-                vc = nv[1][1];
-                int k = 0;
-#pragma unroll
-                for (int a = 0; a < 3; a++)
-#pragma unroll
-                    for (int b = 0; b < 3; b++)
-                        if (a != 1 || b != 1) dv[k++] = psub(nv[a][b], vc);
-                if (kp.ext) fc = G.frc[(uint32_t)cx * (uint32_t)kp.gy + (uint32_t)cy];
-            }
-            // column sums first (weights of y), then the row combination (weights of x),
-            // so that only one axis's weight pairs are live at a time
-            const PT one = pbc(Real(1));
-            PT sa[3], ta[3];
-            {
-                PT wy[3];
-                bspline2(pbc(A.y), wy);
-                const PT ny = pbc(-A.y);
-                const PT gy[3] = {pmul(wy[0], psub(ny, one)), pmul(wy[1], ny), pmul(wy[2], padd(ny, one))};
-                // a = 0: dv[0..2] are nodes (0, 0..2); a = 1: dv[3], dv[4] are nodes (1, 0), (1, 2)
-                // (the centre's difference is zero); a = 2: dv[5..7] are nodes (2, 0..2)
-                sa[0] = pfma(wy[2], dv[2], pfma(wy[1], dv[1], pmul(wy[0], dv[0])));
-                ta[0] = pfma(gy[2], dv[2], pfma(gy[1], dv[1], pmul(gy[0], dv[0])));
-                sa[1] = pfma(wy[2], dv[4], pmul(wy[0], dv[3]));
-                ta[1] = pfma(gy[2], dv[4], pmul(gy[0], dv[3]));
-                sa[2] = pfma(wy[2], dv[7], pfma(wy[1], dv[6], pmul(wy[0], dv[5])));
-                ta[2] = pfma(gy[2], dv[7], pfma(gy[1], dv[6], pmul(gy[0], dv[5])));
-            }
-            PT sv, pv, qv;
-            {
-                PT wx[3];
-                bspline2(pbc(A.x), wx);
-                const PT nx = pbc(-A.x);
-                const PT gx[3] = {pmul(wx[0], psub(nx, one)), pmul(wx[1], nx), pmul(wx[2], padd(nx, one))};
-                sv = pfma(wx[2], sa[2], pfma(wx[1], sa[1], pmul(wx[0], sa[0])));
-                pv = pfma(gx[2], sa[2], pfma(gx[1], sa[1], pmul(gx[0], sa[0])));
-                qv = pfma(wx[2], ta[2], pfma(wx[1], ta[1], pmul(wx[0], ta[0])));
-            }
-            v = padd(vc, sv);
-            const PT fh = pbc(kp.four_h_inv);
-            c0 = pmul(fh, pv);
-            c1 = pmul(fh, qv);
+        const bool act = !(util & kDisabled);
+        if (inb && !act) sg.K[local].x = kNoScatter;
+        if (MODE != FUSED_LEARNED && !act) {
+            if (!inb) break;
+            continue;
         }
-        const PT xy = pfma(v, pbc(kp.dt_h_inv), pmk(A.x, A.y));
-        {   // one test in the usual case; a NaN in any of the sums reaches the total
-            const PT t = padd(padd(v, xy), padd(c0, c1));
-            if (isnan(t.x + t.y)) {
-                if (isnan(v.x + v.y)) err |= kErrVelNan;
-                if (isnan(xy.x + xy.y)) err |= kErrPosNan;
-                if (isnan((c0.x + c0.y) + (c1.x + c1.y))) err |= kErrBpNan;
-            }
-        }
-        Real x = xy.x, y = xy.y;
+        // The learned instance keeps every lane in the loop body (inactive
+        // lanes with act = false), so that the warp meets at the network.
+        Real x = Real(0), y = Real(0), Jp = Real(0), thick = Real(0);
+        M2<Real> H = {Real(0), Real(0), Real(0), Real(0)};
+        int cx = 0, cy = 0;
         bool moved = false;
-        if (x > Real(0.5)) { x -= Real(1); cx++; moved = true; }
-        else if (x < Real(-0.5)) { x += Real(1); cx--; moved = true; }
-        if (y > Real(0.5)) { y -= Real(1); cy++; moved = true; }
-        else if (y < Real(-0.5)) { y += Real(1); cy--; moved = true; }
-        if (moved && (cx <= 1 || cx >= kp.gx - 2 || cy <= 1 || cy >= kp.gy - 2)) {
-            util |= kDisabled;
-            ndis++;
-        }
-        if (x > Real(0.5) || x < Real(-0.5) || y > Real(0.5) || y < Real(-0.5)) err |= kErrJump;
+        PT v = pbc(Real(0)), c0 = pbc(Real(0)), c1 = pbc(Real(0));   // (vx, vy), (c00, c10), (c01, c11)
+        Kin<Real> k{};
+        Real p_tr = Real(0), q_tr = Real(0);
+        SvdH<Real> svd{};
+        bool net = false;   // FUSED_LEARNED: this lane's projection goes to the network
+        if (act) {
+            const V4<Real> A = sg.A[local];
+            const V4<Real> Hv = sg.H[local];
+            Jp = A.z;
+            thick = A.w;
+            H = {Hv.x, Hv.y, Hv.z, Hv.w};
+            cx = (int)(key.x & 0xffff); cy = (int)(key.x >> 16);
+            if (cell_in_range(cx, cy, kp.gx, kp.gy)) {
+                if (!ICEMPM_VEL_CACHE || key.x != vcell) {
+                    vcell = key.x;
+                    const V2<Real> *col = G.vel + ((uint32_t)(cx - 1) * (uint32_t)kp.gy + (uint32_t)(cy - 1));
+                    PT nv[3][3];
+#pragma unroll
+                    for (int a = 0; a < 3; a++)
+#pragma unroll
+                        for (int b = 0; b < 3; b++) nv[a][b] = ld_vel(col + (uint32_t)a * (uint32_t)kp.gy + b);
+                    vc = nv[1][1];
+                    int kd = 0;
+#pragma unroll
+                    for (int a = 0; a < 3; a++)
+#pragma unroll
+                        for (int b = 0; b < 3; b++)
+                            if (a != 1 || b != 1) dv[kd++] = psub(nv[a][b], vc);
+                    if (kp.ext) fc = G.frc[(uint32_t)cx * (uint32_t)kp.gy + (uint32_t)cy];
+                }
+                // column sums first (weights of y), then the row combination (weights of x),
+                // so that only one axis's weight pairs are live at a time
+                const PT one = pbc(Real(1));
+                PT sa[3], ta[3];
+                {
+                    PT wy[3];
+                    bspline2(pbc(A.y), wy);
+                    const PT ny = pbc(-A.y);
+                    const PT gy[3] = {pmul(wy[0], psub(ny, one)), pmul(wy[1], ny), pmul(wy[2], padd(ny, one))};
+                    // a = 0: dv[0..2] are nodes (0, 0..2); a = 1: dv[3], dv[4] are nodes (1, 0), (1, 2)
+                    // (the centre's difference is zero); a = 2: dv[5..7] are nodes (2, 0..2)
+                    sa[0] = pfma(wy[2], dv[2], pfma(wy[1], dv[1], pmul(wy[0], dv[0])));
+                    ta[0] = pfma(gy[2], dv[2], pfma(gy[1], dv[1], pmul(gy[0], dv[0])));
+                    sa[1] = pfma(wy[2], dv[4], pmul(wy[0], dv[3]));
+                    ta[1] = pfma(gy[2], dv[4], pmul(gy[0], dv[3]));
+                    sa[2] = pfma(wy[2], dv[7], pfma(wy[1], dv[6], pmul(wy[0], dv[5])));
+                    ta[2] = pfma(gy[2], dv[7], pfma(gy[1], dv[6], pmul(gy[0], dv[5])));
+                }
+                PT sv, pv, qv;
+                {
+                    PT wx[3];
+                    bspline2(pbc(A.x), wx);
+                    const PT nx = pbc(-A.x);
+                    const PT gx[3] = {pmul(wx[0], psub(nx, one)), pmul(wx[1], nx), pmul(wx[2], padd(nx, one))};
+                    sv = pfma(wx[2], sa[2], pfma(wx[1], sa[1], pmul(wx[0], sa[0])));
+                    pv = pfma(gx[2], sa[2], pfma(gx[1], sa[1], pmul(gx[0], sa[0])));
+                    qv = pfma(wx[2], ta[2], pfma(wx[1], ta[1], pmul(wx[0], ta[0])));
+                }
+                v = padd(vc, sv);
+                const PT fh = pbc(kp.four_h_inv);
+                c0 = pmul(fh, pv);
+                c1 = pmul(fh, qv);
+            }
+            const PT xy = pfma(v, pbc(kp.dt_h_inv), pmk(A.x, A.y));
+            {   // one test in the usual case; a NaN in any of the sums reaches the total
+                const PT t = padd(padd(v, xy), padd(c0, c1));
+                if (isnan(t.x + t.y)) {
+                    if (isnan(v.x + v.y)) err |= kErrVelNan;
+                    if (isnan(xy.x + xy.y)) err |= kErrPosNan;
+                    if (isnan((c0.x + c0.y) + (c1.x + c1.y))) err |= kErrBpNan;
+                }
+            }
+            x = xy.x; y = xy.y;
+            if (x > Real(0.5)) { x -= Real(1); cx++; moved = true; }
+            else if (x < Real(-0.5)) { x += Real(1); cx--; moved = true; }
+            if (y > Real(0.5)) { y -= Real(1); cy++; moved = true; }
+            else if (y < Real(-0.5)) { y += Real(1); cy--; moved = true; }
+            if (moved && (cx <= 1 || cx >= kp.gx - 2 || cy <= 1 || cy >= kp.gy - 2)) {
+                util |= kDisabled;
+                ndis++;
+            }
+            if (x > Real(0.5) || x < Real(-0.5) || y > Real(0.5) || y < Real(-0.5)) err |= kErrJump;
 
-        // Fe <- (I + dt C) Fe, i.e. H <- H + D + D H with D = dt C
-        {
-            const Real d00 = kp.dt * c0.x, d01 = kp.dt * c1.x, d10 = kp.dt * c0.y, d11 = kp.dt * c1.y;
-            const M2<Real> h = H;
-            H.a00 = h.a00 + d00 + (d00 * h.a00 + d01 * h.a10);
-            H.a01 = h.a01 + d01 + (d00 * h.a01 + d01 * h.a11);
-            H.a10 = h.a10 + d10 + (d10 * h.a00 + d11 * h.a10);
-            H.a11 = h.a11 + d11 + (d10 * h.a01 + d11 * h.a11);
-        }
-        if (isnan((H.a00 + H.a10) + (H.a01 + H.a11))) err |= kErrFeNan;
-        Kin<Real> k = kinematics(H);
-        Real p_tr, q_tr;
-        pq(k, kp.mat.mu, kp.mat.kappa, p_tr, q_tr);
-        if (!(util & kCrushed)) util = failure_check(kp.mat, util, p_tr, q_tr);
-        if (util & kCrushed) {
-            const SvdH<Real> svd = svd_h(H);
-            const Real jp0 = Jp;
-            wolper_dp(kp.mat, thick, p_tr, q_tr, k, svd, H, Jp);
-            if (HARVEST && kp.harvest && (i + (uint32_t)step) % (uint32_t)kp.harvest_stride == 0u)
-                harvest_record(kp.harvest, kp.mat, svd, p_tr, q_tr, jp0, thick, H, Jp);
+            // Fe <- (I + dt C) Fe, i.e. H <- H + D + D H with D = dt C
+            {
+                const Real d00 = kp.dt * c0.x, d01 = kp.dt * c1.x, d10 = kp.dt * c0.y, d11 = kp.dt * c1.y;
+                const M2<Real> h = H;
+                H.a00 = h.a00 + d00 + (d00 * h.a00 + d01 * h.a10);
+                H.a01 = h.a01 + d01 + (d00 * h.a01 + d01 * h.a11);
+                H.a10 = h.a10 + d10 + (d10 * h.a00 + d11 * h.a10);
+                H.a11 = h.a11 + d11 + (d10 * h.a01 + d11 * h.a11);
+            }
             if (isnan((H.a00 + H.a10) + (H.a01 + H.a11))) err |= kErrFeNan;
             k = kinematics(H);
-        }
-
-        V4<Real> Ao; Ao.x = x; Ao.y = y; Ao.z = Jp; Ao.w = thick;
-        st_stream(P.A + i, Ao);
-        V4<Real> Ho; Ho.x = H.a00; Ho.y = H.a01; Ho.z = H.a10; Ho.w = H.a11;
-        st_stream(P.H + i, Ho);
-        if (store_vc || (util & kDisabled)) {   // a point disabled now keeps this step's V and C
-            V2<Real> Vo; Vo.x = v.x; Vo.y = v.y;
-            st_stream(P.V + i, Vo);
-            V4<Real> Co; Co.x = c0.x; Co.y = c1.x; Co.z = c0.y; Co.w = c1.y;
-            st_stream(P.C + i, Co);
-        }
-        const uint32_t cell = ((uint32_t)cy << 16) | (uint32_t)cx;   // as kernels.cuh:305
-        if (moved || util != key.y) {
-            uint2 ko; ko.x = moved ? cell : key.x; ko.y = util;
-            st_stream(P.K + i, ko);
-        }
-        if (recordPQ) { V2<Real> pqv; pqv.x = p_tr; pqv.y = q_tr; st_stream(P.PQ + i, pqv); }
-
-        // P2G source of the new state (make_src in pair form): with
-        // S = m_p C - dt_vol_Dpinv Jp_inv thickness tau (columns S0, S1),
-        // A = m_p v - h (S0 x + S1 y) (+ the extended forcing's impulse).
-        uint2 src_key = make_uint2(kNoScatter, 0u);   // new cell and mass of the source, or no scatter
-        if (!(util & kDisabled)) {
-            if (cell_in_range(cx, cy, kp.gx, kp.gy)) {
-                const M2<Real> tau = kirchhoff(k, kp.mat.mu, kp.mat.kappa);
-                const Real mp = kp.particle_mass * thick;
-                const PT nsc = pbc(-(kp.dt_vol_Dpinv * Jp * thick)), mpp = pbc(mp);
-                const PT S0 = pfma(mpp, c0, pmul(nsc, pmk(tau.a00, tau.a10)));
-                const PT S1 = pfma(mpp, c1, pmul(nsc, pmk(tau.a01, tau.a11)));
-                PT Av = pfma(pbc(-kp.h), pfma(S0, pbc(x), pmul(S1, pbc(y))), pmul(mpp, v));
-                if (kp.ext) {   // wind stress and current of the new cell's node
-                    const V4<Real> f = moved ? G.frc[(uint32_t)cx * (uint32_t)kp.gy + (uint32_t)cy] : fc;
-                    const PT d = psub(pmk(f.x, f.y), v);
-                    const Real cw = kp.rho_w_cd * tsqrt(d.x * d.x + d.y * d.y);
-                    Av = pfma(pbc(kp.ext_impulse), pfma(pbc(cw), d, pmk(f.z, f.w)), Av);
+            pq(k, kp.mat.mu, kp.mat.kappa, p_tr, q_tr);
+            if (!(util & kCrushed)) util = failure_check(kp.mat, util, p_tr, q_tr);
+            if (util & kCrushed) {
+                svd = svd_h(H);
+                if (MODE == FUSED_LEARNED && kp.mlp && is_projection(kp.mat, p_tr, q_tr) && thick > Real(0) &&
+                    Jp > Real(0) && svd.e1 > Real(-1)) {
+                    net = true;
+                } else {
+                    const Real jp0 = Jp;
+                    wolper_dp(kp.mat, thick, p_tr, q_tr, k, svd, H, Jp);
+                    if (MODE == FUSED_HARVEST && kp.harvest && (i + (uint32_t)step) % (uint32_t)kp.harvest_stride == 0u)
+                        harvest_record(kp.harvest, kp.mat, svd, p_tr, q_tr, jp0, thick, H, Jp);
+                    if (isnan((H.a00 + H.a10) + (H.a01 + H.a11))) err |= kErrFeNan;
+                    k = kinematics(H);
                 }
-                const Real fm = FIXED ? Real(kp.scale_m) : Real(1);
-                const Real fp = FIXED ? Real(kp.scale_p) : Real(1);
-                const PT hp = pbc(kp.h * fp);
-                const PT sA = pmul(Av, pbc(fp)), sS0 = pmul(hp, S0), sS1 = pmul(hp, S1);
-                const Real smp = mp * fm;
-                // Fixed point: a node term is at most max(w) <= 0.5625 times the
-                // bounds below.  Finite sources with |x|, |y| <= 2 raise no P2G
-                // bit; anything else takes the exact tests.
-                const Real lim_p = FIXED ? Real(kp.lim_p) : Real(sizeof(Real) == 4 ? 1e30 : 1e300);
-                const Real lim_m = FIXED ? Real(kp.lim_m) : lim_p;
-                const Real bx = fabs(Av.x) + kp.h * (fabs(S0.x) + fabs(S1.x));
-                const Real by = fabs(Av.y) + kp.h * (fabs(S0.y) + fabs(S1.y));
-                if (!(bx <= lim_p && by <= lim_p && mp <= lim_m && fabs(x) <= Real(2) && fabs(y) <= Real(2))) {
-                    if (FIXED && (!(bx <= Real(kp.lim_p)) || !(by <= Real(kp.lim_p)) || !(mp <= Real(kp.lim_m))))
-                        perr |= kErrFixedOverflow;
-                    Real wxs[3], wys[3];
-                    bspline(x, wxs);
-                    bspline(y, wys);
-                    const Real sw = (wxs[0] + wxs[1] + wxs[2]) + (wys[0] + wys[1] + wys[2]);
-                    if (isnan(sw + smp)) perr |= kErrP2gNanMass;
-                    if (isnan(sw + ((sA.x + sA.y) + (sS0.x + sS1.x) + (sS0.y + sS1.y)))) perr |= kErrP2gNanVel;
-                }
-                V4<Real> a4; a4.x = x; a4.y = y; a4.z = sS1.x; a4.w = sS1.y;
-                sg.A[local] = a4;
-                V4<Real> h4; h4.x = sA.x; h4.y = sA.y; h4.z = sS0.x; h4.w = sS0.y;
-                sg.H[local] = h4;
-                src_key.x = cell;
-                src_key.y = put_src_mass(sg, local, smp);
-                xmn = min(xmn, (unsigned)cx); ymn = min(ymn, (unsigned)cy);
-                xmx = max(xmx, (unsigned)cx); ymx = max(ymx, (unsigned)cy);
-                any = true;
-            } else {
-                perr |= kErrLeftArea;
             }
         }
+        if constexpr (MODE == FUSED_LEARNED) {
+            if (__any_sync(0xffffffffu, net)) {
+                learned_projection<Real>(kp, *ml, wid, lane, net, thick, p_tr, q_tr, svd, k, H, Jp);
+                if (net) {
+                    if (isnan((H.a00 + H.a10) + (H.a01 + H.a11))) err |= kErrFeNan;
+                    k = kinematics(H);
+                }
+            }
+        }
+        if (!act) continue;
+
+            V4<Real> Ao; Ao.x = x; Ao.y = y; Ao.z = Jp; Ao.w = thick;
+            st_stream(P.A + i, Ao);
+            V4<Real> Ho; Ho.x = H.a00; Ho.y = H.a01; Ho.z = H.a10; Ho.w = H.a11;
+            st_stream(P.H + i, Ho);
+            if (store_vc || (util & kDisabled)) {   // a point disabled now keeps this step's V and C
+                V2<Real> Vo; Vo.x = v.x; Vo.y = v.y;
+                st_stream(P.V + i, Vo);
+                V4<Real> Co; Co.x = c0.x; Co.y = c1.x; Co.z = c0.y; Co.w = c1.y;
+                st_stream(P.C + i, Co);
+            }
+            const uint32_t cell = ((uint32_t)cy << 16) | (uint32_t)cx;   // as kernels.cuh:305
+            if (moved || util != key.y) {
+                uint2 ko; ko.x = moved ? cell : key.x; ko.y = util;
+                st_stream(P.K + i, ko);
+            }
+            if (recordPQ) { V2<Real> pqv; pqv.x = p_tr; pqv.y = q_tr; st_stream(P.PQ + i, pqv); }
+
+            // P2G source of the new state (make_src in pair form): with
+            // S = m_p C - dt_vol_Dpinv Jp_inv thickness tau (columns S0, S1),
+            // A = m_p v - h (S0 x + S1 y) (+ the extended forcing's impulse).
+            uint2 src_key = make_uint2(kNoScatter, 0u);   // new cell and mass of the source, or no scatter
+            if (!(util & kDisabled)) {
+                if (cell_in_range(cx, cy, kp.gx, kp.gy)) {
+                    const M2<Real> tau = kirchhoff(k, kp.mat.mu, kp.mat.kappa);
+                    const Real mp = kp.particle_mass * thick;
+                    const PT nsc = pbc(-(kp.dt_vol_Dpinv * Jp * thick)), mpp = pbc(mp);
+                    const PT S0 = pfma(mpp, c0, pmul(nsc, pmk(tau.a00, tau.a10)));
+                    const PT S1 = pfma(mpp, c1, pmul(nsc, pmk(tau.a01, tau.a11)));
+                    PT Av = pfma(pbc(-kp.h), pfma(S0, pbc(x), pmul(S1, pbc(y))), pmul(mpp, v));
+                    if (kp.ext) {   // wind stress and current of the new cell's node
+                        const V4<Real> f = moved ? G.frc[(uint32_t)cx * (uint32_t)kp.gy + (uint32_t)cy] : fc;
+                        const PT d = psub(pmk(f.x, f.y), v);
+                        const Real cw = kp.rho_w_cd * tsqrt(d.x * d.x + d.y * d.y);
+                        Av = pfma(pbc(kp.ext_impulse), pfma(pbc(cw), d, pmk(f.z, f.w)), Av);
+                    }
+                    const Real fm = FIXED ? Real(kp.scale_m) : Real(1);
+                    const Real fp = FIXED ? Real(kp.scale_p) : Real(1);
+                    const PT hp = pbc(kp.h * fp);
+                    const PT sA = pmul(Av, pbc(fp)), sS0 = pmul(hp, S0), sS1 = pmul(hp, S1);
+                    const Real smp = mp * fm;
+                    // Fixed point: a node term is at most max(w) <= 0.5625 times the
+                    // bounds below.  Finite sources with |x|, |y| <= 2 raise no P2G
+                    // bit; anything else takes the exact tests.
+                    const Real lim_p = FIXED ? Real(kp.lim_p) : Real(sizeof(Real) == 4 ? 1e30 : 1e300);
+                    const Real lim_m = FIXED ? Real(kp.lim_m) : lim_p;
+                    const Real bx = fabs(Av.x) + kp.h * (fabs(S0.x) + fabs(S1.x));
+                    const Real by = fabs(Av.y) + kp.h * (fabs(S0.y) + fabs(S1.y));
+                    if (!(bx <= lim_p && by <= lim_p && mp <= lim_m && fabs(x) <= Real(2) && fabs(y) <= Real(2))) {
+                        if (FIXED && (!(bx <= Real(kp.lim_p)) || !(by <= Real(kp.lim_p)) || !(mp <= Real(kp.lim_m))))
+                            perr |= kErrFixedOverflow;
+                        Real wxs[3], wys[3];
+                        bspline(x, wxs);
+                        bspline(y, wys);
+                        const Real sw = (wxs[0] + wxs[1] + wxs[2]) + (wys[0] + wys[1] + wys[2]);
+                        if (isnan(sw + smp)) perr |= kErrP2gNanMass;
+                        if (isnan(sw + ((sA.x + sA.y) + (sS0.x + sS1.x) + (sS0.y + sS1.y)))) perr |= kErrP2gNanVel;
+                    }
+                    V4<Real> a4; a4.x = x; a4.y = y; a4.z = sS1.x; a4.w = sS1.y;
+                    sg.A[local] = a4;
+                    V4<Real> h4; h4.x = sA.x; h4.y = sA.y; h4.z = sS0.x; h4.w = sS0.y;
+                    sg.H[local] = h4;
+                    src_key.x = cell;
+                    src_key.y = put_src_mass(sg, local, smp);
+                    xmn = min(xmn, (unsigned)cx); ymn = min(ymn, (unsigned)cy);
+                    xmx = max(xmx, (unsigned)cx); ymx = max(ymx, (unsigned)cy);
+                    any = true;
+                } else {
+                    perr |= kErrLeftArea;
+                }
+            }
         sg.K[local] = src_key;
     }
     fence_proxy_async_smem();
@@ -1292,8 +1532,15 @@ __device__ __forceinline__ void fused_chunk(ChunkSmem<Real, Acc, BT, PPT, CAP, S
     }
 }
 
-template <class Real, class Acc, int BT, int PPT, int CAP, int STAGES, bool HARVEST>
-__global__ void __launch_bounds__(BT, (sizeof(Real) == 8 ? 1 : ICEMPM_FUSED_MINB))
+// Dynamic shared memory of an instance of the fused kernel: the chunk stages
+// (and tile), and for the learned instance the network after them.
+template <class SM, int BT, int MODE> constexpr size_t fused_smem_bytes()
+{
+    return MODE == FUSED_LEARNED ? (sizeof(SM) + 15) / 16 * 16 + sizeof(mlp::Smem<BT / 32>) : sizeof(SM);
+}
+
+template <class Real, class Acc, int BT, int PPT, int CAP, int STAGES, int MODE>
+__global__ void __launch_bounds__(BT, (sizeof(Real) == 8 ? 1 : (MODE == FUSED_LEARNED ? 4 : ICEMPM_FUSED_MINB)))
 k_g2p_p2g(KParams<Real> kp, Pts<Real> P, Grid<Real, Acc> G, DevStatus *st, int n, int nchunks)
 {
     static_assert(STAGES == 1 || STAGES == 2, "one or two stages");
@@ -1302,6 +1549,11 @@ k_g2p_p2g(KParams<Real> kp, Pts<Real> P, Grid<Real, Acc> G, DevStatus *st, int n
     extern __shared__ __align__(128) unsigned char smem_raw[];
     SM &sm = *reinterpret_cast<SM *>(smem_raw);
     const int tid = threadIdx.x;
+    mlp::Smem<BT / 32> *ml = nullptr;
+    if constexpr (MODE == FUSED_LEARNED) {   // launched only with a network (kp.mlp)
+        ml = reinterpret_cast<mlp::Smem<BT / 32> *>(smem_raw + (sizeof(SM) + 15) / 16 * 16);
+        mlp::load_packed(ml->p, kp.mlp, tid, BT);
+    }
 
     if (tid == 0) {
         mbar_init(&sm.mbar[0], 1);
@@ -1335,8 +1587,8 @@ k_g2p_p2g(KParams<Real> kp, Pts<Real> P, Grid<Real, Acc> G, DevStatus *st, int n
         const uint32_t base_n = (uint32_t)(c + (int)gridDim.x) * CH;
         if (STAGES == 2 && tid == 0 && next)
             fetch_chunk(sm.stage[s ^ 1], P, base_n, CH, &sm.mbar[s ^ 1], kp.tx_extra);
-        fused_chunk<Real, Acc, BT, PPT, CAP, STAGES, HARVEST>(sm, s, kp, P, G, (uint32_t)c * CH, n, step, recordPQ, store_vc,
-                                                     next, P, base_n, err, perr, ndis);
+        fused_chunk<Real, Acc, BT, PPT, CAP, STAGES, MODE>(sm, s, kp, P, G, (uint32_t)c * CH, n, step, recordPQ, store_vc,
+                                                  next, P, base_n, err, perr, ndis, ml);
     }
     warp_flush_status(st, err, perr, ndis);
 
@@ -1441,8 +1693,8 @@ k_g2p_p2g_batch(const SceneDesc<Real, Acc> *__restrict__ scenes, const int *__re
         const uint32_t base_n = (uint32_t)(cn - Sn.chunk0) * CH;
         if (STAGES == 2 && tid == 0 && next) fetch_chunk(sm.stage[s ^ 1], Sn.P, base_n, CH, &sm.mbar[s ^ 1]);
         const bool recordPQ = S.kp.update_every > 0 && (step % S.kp.update_every) == 0;
-        fused_chunk<Real, Acc, BT, PPT, CAP, STAGES, false>(sm, s, S.kp, S.P, S.G, (uint32_t)(c - S.chunk0) * CH, S.n, step,
-                                                     recordPQ, store_vc, next, Sn.P, base_n, err, perr, ndis);
+        fused_chunk<Real, Acc, BT, PPT, CAP, STAGES, FUSED_PLAIN>(sm, s, S.kp, S.P, S.G, (uint32_t)(c - S.chunk0) * CH, S.n,
+                                                          step, recordPQ, store_vc, next, Sn.P, base_n, err, perr, ndis);
         warp_flush_status(S.st, err, perr, ndis);
     }
 

@@ -123,10 +123,19 @@ public:
         tile_.tx = 8; tile_.ty = BT * PPT / 32;
         tile_.ntiles_y = (gy_ + tile_.ty - 1) / tile_.ty;
         // persistent grid of the fused kernel: as many CTAs as fit on the device
-        auto kern = k_g2p_p2g<Real, Acc, BT, PPT, CAP, STAGES, false>;
+        auto kern = k_g2p_p2g<Real, Acc, BT, PPT, CAP, STAGES, FUSED_PLAIN>;
         ICEMPM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(FusedSmem)));
-        ICEMPM_CUDA(cudaFuncSetAttribute(k_g2p_p2g<Real, Acc, BT, PPT, CAP, STAGES, true>,
+        ICEMPM_CUDA(cudaFuncSetAttribute(k_g2p_p2g<Real, Acc, BT, PPT, CAP, STAGES, FUSED_HARVEST>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(FusedSmem)));
+        if constexpr (sizeof(Real) == 4) {
+            auto lk = k_g2p_p2g<Real, Acc, BT, PPT, CAP, STAGES, FUSED_LEARNED>;
+            const int lb = (int)fused_smem_bytes<FusedSmem, BT, FUSED_LEARNED>();
+            ICEMPM_CUDA(cudaFuncSetAttribute(lk, cudaFuncAttributeMaxDynamicSharedMemorySize, lb));
+            int lper = 0, lsms = 0;
+            ICEMPM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&lper, lk, BT, lb));
+            ICEMPM_CUDA(cudaDeviceGetAttribute(&lsms, cudaDevAttrMultiProcessorCount, o.device));
+            learned_ctas_ = lper * lsms;
+        }
         int per_sm = 0, sms = 0;
         ICEMPM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, BT, sizeof(FusedSmem)));
         ICEMPM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, o.device));
@@ -403,19 +412,50 @@ public:
     {
         const int nchunks = (int)(((size_t)n_ + CH - 1) / CH);
         const unsigned nb = (unsigned)(ICEMPM_FUSED_PERSIST ? std::min(nchunks, fused_ctas_) : nchunks);
-        if (kp_.harvest)
-            k_g2p_p2g<Real, Acc, BT, PPT, CAP, STAGES, true>
+        bool learned = false;
+        if constexpr (sizeof(Real) == 4) {
+            if (kp_.mlp && learned_ctas_ > 0) {
+                const unsigned lnb = (unsigned)(ICEMPM_FUSED_PERSIST ? std::min(nchunks, learned_ctas_) : nchunks);
+                k_g2p_p2g<Real, Acc, BT, PPT, CAP, STAGES, FUSED_LEARNED>
+                    <<<lnb, BT, fused_smem_bytes<FusedSmem, BT, FUSED_LEARNED>(), stream_>>>(kp_, pts_[par_], grid(), st_,
+                                                                                          (int)n_, nchunks);
+                learned = true;
+            }
+        }
+        if (learned) {
+        } else if (kp_.harvest)
+            k_g2p_p2g<Real, Acc, BT, PPT, CAP, STAGES, FUSED_HARVEST>
                 <<<nb, BT, sizeof(FusedSmem), stream_>>>(kp_, pts_[par_], grid(), st_, (int)n_, nchunks);
         else
-            k_g2p_p2g<Real, Acc, BT, PPT, CAP, STAGES, false>
+            k_g2p_p2g<Real, Acc, BT, PPT, CAP, STAGES, FUSED_PLAIN>
                 <<<nb, BT, sizeof(FusedSmem), stream_>>>(kp_, pts_[par_], grid(), st_, (int)n_, nchunks);
         launches_++;
     }
+    // The plain FP32 baseline (ICEMPM_VARIANT_TEXTBOOK): three plain kernels
+    // per sub-step instead of the fused one (k_textbook_p2g / k_textbook_g2p).
+    bool textbook() const { return std::is_same<Acc, float>::value && opts_.variant == ICEMPM_VARIANT_TEXTBOOK; }
+
+    void launch_textbook(bool prime_only)
+    {
+        if constexpr (std::is_same<Acc, float>::value) {
+            const unsigned nb = (unsigned)((n_ + 255) / 256);
+            if (!prime_only) {
+                k_textbook_g2p<Real><<<nb, 256, 0, stream_>>>(kp_, pts_[par_], grid(), st_, (int)n_);
+                launches_++;
+            }
+            k_textbook_p2g<Real><<<nb, 256, 0, stream_>>>(kp_, pts_[par_], grid(), st_, (int)n_, prime_only ? 0 : 1);
+            launches_++;
+        }
+    }
+
     int prime()
     {
         ICEMPM_CUDA(cudaMemsetAsync(acc_, 0, 3 * Gp_ * sizeof(Acc), stream_));
         ICEMPM_CUDA(cudaMemsetAsync(&st_->err_pending, 0, sizeof(uint32_t), stream_));
-        if (n_ > 0) {
+        if (n_ > 0 && textbook()) {
+            launch_textbook(true);
+            ICEMPM_CUDA(cudaGetLastError());
+        } else if (n_ > 0) {
             const unsigned nb = (n_ + BT_P2G - 1) / BT_P2G;
             k_p2g<Real, Acc, BT_P2G, CAP_P2G><<<nb, BT_P2G, 0, stream_>>>(kp_, pts_[par_], grid(), st_, (int)n_);
             launches_++;
@@ -429,10 +469,16 @@ public:
     {
         for (int s = 0; s < k; s++) {
             launch_update();
-            if (n_ > 0) launch_fused();
+            if (n_ > 0) launch_step_points();
         }
         ICEMPM_CUDA(cudaGetLastError());
         return 0;
+    }
+
+    void launch_step_points()
+    {
+        if (textbook()) launch_textbook(false);
+        else launch_fused();
     }
 
     int run_chunk_graph()
@@ -444,7 +490,7 @@ public:
             const uint64_t before = launches_;
             for (int s = 0; s < GRAPH_STEPS; s++) {
                 launch_update();
-                if (n_ > 0) launch_fused();
+                if (n_ > 0) launch_step_points();
             }
             graph_launches_ = launches_ - before;
             launches_ = before;
@@ -501,6 +547,46 @@ public:
 
     // Device time between the event pair around the last icempm_step or
     // icempm_phase_times call, and the locality-sort time inside it.
+    // Sort cadence on the live scene, which therefore advances (step indices
+    // from first_step): trial_steps sub-steps in the current order, one
+    // locality sort (timed), trial_steps sub-steps in the sorted order; a
+    // cadence k in {100, 400} is kept when sorted ms/step + sort ms / k beats
+    // the current order's ms/step, else 0 (sort only at upload and
+    // compaction).  The choice becomes the context's sort_every.
+    int tune_sort(int trial_steps, int first_step, int32_t *sort_every) override
+    {
+        if (trial_steps <= 0) return fail(ICEMPM_E_ARG, "trial_steps must be > 0");
+        opts_.sort_every = 0;
+        int rc = step(trial_steps, first_step);
+        if (rc) return rc;
+        float ms[4];
+        rc = timings(ms);
+        if (rc) return rc;
+        const float unsorted = ms[0] / (float)trial_steps;
+        ICEMPM_CUDA(cudaEventRecord(evs_[0], stream_));
+        rc = locality_sort();
+        if (rc) return rc;
+        ICEMPM_CUDA(cudaEventRecord(evs_[1], stream_));
+        ICEMPM_CUDA(cudaEventSynchronize(evs_[1]));
+        float sort_ms = 0;
+        ICEMPM_CUDA(cudaEventElapsedTime(&sort_ms, evs_[0], evs_[1]));
+        rc = step(trial_steps, first_step + trial_steps);
+        if (rc) return rc;
+        rc = timings(ms);
+        if (rc) return rc;
+        const float sorted = ms[0] / (float)trial_steps;
+        float best = unsorted;
+        int k_best = 0;
+        for (int k : {100, 400}) {
+            const float est = sorted + sort_ms / (float)k;
+            if (est < best) { best = est; k_best = k; }
+        }
+        opts_.sort_every = k_best;
+        steps_since_sort_ = trial_steps;
+        if (sort_every) *sort_every = k_best;
+        return 0;
+    }
+
     int timings(float ms[4]) override
     {
         ms[0] = ms[1] = ms[2] = ms[3] = 0;
@@ -525,7 +611,7 @@ public:
             cudaEventRecord(ev[3 * s], stream_);
             launch_update();
             cudaEventRecord(ev[3 * s + 1], stream_);
-            if (n_ > 0) launch_fused();
+            if (n_ > 0) launch_step_points();
             cudaEventRecord(ev[3 * s + 2], stream_);
         }
         ICEMPM_CUDA(cudaEventRecord(ev1_, stream_));
@@ -771,6 +857,46 @@ public:
     double fixed_scale_p() const override { return kp_.scale_p; }
 
 private:
+    // The learned return map on the step path (FP32 state only): the FP32
+    // parameters and normalisation (device pointers) are packed for the
+    // fused kernel, whose projections onto the yield surface then go to the
+    // network, with the exact map as fallback above `tol`.  Null params: off.
+    int set_learned_map(const float *d_params, const float *d_norm, float tol) override
+    {
+        if (sizeof(Real) != 4 || textbook())
+            return fail(ICEMPM_E_UNSUPPORTED, "the learned return map needs the fused FP32-state variants");
+        if (!d_params) {
+            kp_.mlp = nullptr;
+            invalidate_graphs();
+            return 0;
+        }
+        if (!d_norm || !(tol > 0.0f)) return fail(ICEMPM_E_ARG, "norm must be given and tol > 0");
+        if (learned_ctas_ < 1) return fail(ICEMPM_E_UNSUPPORTED, "the learned fused kernel does not fit on one SM");
+        if (!mlp_packed_) ICEMPM_CUDA(cudaMalloc(&mlp_packed_, mlp_packed_bytes()));
+        if (!mlp_counts_) ICEMPM_CUDA(cudaMalloc(&mlp_counts_, 2 * sizeof(unsigned long long)));
+        int rc = mlp_pack(d_params, d_norm, mlp_packed_, stream_);
+        if (rc) return rc;
+        ICEMPM_CUDA(cudaMemsetAsync(mlp_counts_, 0, 2 * sizeof(unsigned long long), stream_));
+        ICEMPM_CUDA(cudaStreamSynchronize(stream_));
+        kp_.mlp = static_cast<const mlp::Packed *>(mlp_packed_);
+        kp_.mlp_tol = tol;
+        kp_.mlp_counts = mlp_counts_;
+        invalidate_graphs();
+        return 0;
+    }
+
+    int learned_counts(uint64_t *kept, uint64_t *fallbacks) override
+    {
+        unsigned long long h[2] = {0, 0};
+        if (mlp_counts_) {
+            ICEMPM_CUDA(cudaMemcpyAsync(h, mlp_counts_, sizeof(h), cudaMemcpyDeviceToHost, stream_));
+            ICEMPM_CUDA(cudaStreamSynchronize(stream_));
+        }
+        if (kept) *kept = h[0];
+        if (fallbacks) *fallbacks = h[1];
+        return 0;
+    }
+
     int harvest_free()
     {
         if (stream_) ICEMPM_CUDA(cudaStreamSynchronize(stream_));
@@ -799,7 +925,7 @@ private:
         invalidate_graphs();
         cudaFree(pts_mem_); cudaFree(acc_); cudaFree(vel_); cudaFree(cur_); cudaFree(frc_); cudaFree(status_);
         cudaFree(force_); cudaFree(st_); cudaFree(stage_); cudaFree(keys_[0]); cudaFree(keys_[1]);
-        cudaFree(vals_[0]); cudaFree(vals_[1]); cudaFree(sort_tmp_); cudaFree(harvest_); cudaFree(harvest_rec_); cudaFree(frame_mem_); cudaFree(colors_); cudaFree(runs_); cudaFree(aux_);
+        cudaFree(vals_[0]); cudaFree(vals_[1]); cudaFree(sort_tmp_); cudaFree(harvest_); cudaFree(harvest_rec_); cudaFree(mlp_packed_); cudaFree(mlp_counts_); cudaFree(frame_mem_); cudaFree(colors_); cudaFree(runs_); cudaFree(aux_);
         cudaFree(flow_ab_); cudaFree((void *)wind_.w);
         if (ev0_) cudaEventDestroy(ev0_);
         if (ev1_) cudaEventDestroy(ev1_);
@@ -857,6 +983,9 @@ private:
     size_t sort_tmp_bytes_ = 0;
     TileKey tile_{8, 8, 1};
     KParams<Real> kp_{};
+    void *mlp_packed_ = nullptr;                  // the learned map's packed network
+    unsigned long long *mlp_counts_ = nullptr;    // its answers kept / exact fallbacks
+    int learned_ctas_ = 0;                        // persistent grid of the learned instance
     uint32_t tx_extra_ = 0;
     unsigned long long wait_ns_ = kWaitLimitNs;
     bool primed_ = false, timed_ = false;

@@ -11,6 +11,12 @@ namespace icempm {
 // Records `msg` as the calling thread's last error and returns `code`.
 int fail(int code, const std::string &msg);
 
+// The learned return map's network packed for the in-kernel evaluation
+// (surrogate.cu): FP32 parameters and normalisation (device pointers) into
+// a device buffer of mlp_packed_bytes().
+int mlp_pack(const float *d_params, const float *d_norm, void *d_packed, cudaStream_t stream);
+size_t mlp_packed_bytes();
+
 class Engine {
 public:
     virtual ~Engine() {}
@@ -43,6 +49,9 @@ public:
     virtual int set_forcing_time(double tc, double tw) = 0;
     virtual int get_forcing(double *cur, double *stress) = 0;
     virtual int set_barrier_test(uint32_t extra_bytes, uint32_t wait_us) = 0;
+    virtual int set_learned_map(const float *d_params, const float *d_norm, float tol) = 0;
+    virtual int learned_counts(uint64_t *kept, uint64_t *fallbacks) = 0;
+    virtual int tune_sort(int trial_steps, int first_step, int32_t *sort_every) = 0;
 };
 
 // Ensemble of contexts of one variant stepped together (batch.cuh).

@@ -1,0 +1,145 @@
+// mlp_device.cuh -- the learned return map's network inside other kernels.
+//
+// The MLP 4 -> 64 -> 64 -> 3 with SiLU (parameters: see surrogate.cu) is
+// evaluated by one warp on the 32 rows its lanes hold, with BF16 tensor-core
+// MMAs (mma.sync m16n8k16, FP32 accumulate): rows 0-15 and 16-31 are two
+// m-tiles, the 64 hidden features eight n-tiles, and each layer's FP32
+// outputs become, after the activation, the BF16 A fragments of the next
+// layer in registers.  The weights sit in shared memory as BF16 pairs in the
+// B-fragment order (row n of W holds k, k+1 in one word), packed once per
+// network by k_mlp_pack.
+#pragma once
+#include <cstdint>
+#include <cuda_bf16.h>
+
+namespace icempm {
+namespace mlp {
+
+constexpr int IN = 4, HID = 64, OUT = 3;
+// FP32 master parameters, row-major W[out][in]
+constexpr int W1 = 0, B1 = W1 + HID * IN, W2 = B1 + HID, B2 = W2 + HID * HID, W3 = B2 + HID, B3 = W3 + OUT * HID;
+constexpr int NPARAM = B3 + OUT;   // 4675
+
+// The packed network: what a CTA copies into shared memory.
+struct alignas(16) Packed {
+    uint32_t w1[HID][8];      // W1 as BF16 pairs, K padded 4 -> 16
+    uint32_t w2[HID][HID / 2];
+    uint32_t w3[8][HID / 2];  // N padded 3 -> 8
+    float b1[HID], b2[HID], b3[8];
+    float norm[16];           // x mean[4], x std[4], y mean[3], y std[3], 2 unused
+};
+static_assert(sizeof(Packed) % 16 == 0, "16-byte copies");
+
+// Shared memory of the in-kernel network: the packed weights and one row
+// exchange area (32 rows x 4 floats) per warp.
+template <int NWARPS> struct Smem {
+    Packed p;
+    float io[NWARPS][32][4];
+};
+
+__device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi)
+{
+    const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<const uint32_t *>(&v);
+}
+
+__device__ __forceinline__ void mma_bf16_16816(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1)
+{
+    asm volatile("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+                 "{%0,%1,%2,%3};"
+                 : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+                 : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// SiLU z sigmoid(z) = z/2 (1 + tanh(z/2)), with the hardware tanh
+// approximation (relative error ~2^-11, below the BF16 rounding that follows).
+__device__ __forceinline__ float silu_fast(float z)
+{
+    float t;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(0.5f * z));
+    return 0.5f * z * (1.0f + t);
+}
+
+// Copies the packed network into shared memory (all threads of the CTA; a
+// barrier must follow before use).
+__device__ __forceinline__ void load_packed(Packed &dst, const Packed *src, int tid, int nthreads)
+{
+    const uint4 *s = reinterpret_cast<const uint4 *>(src);
+    uint4 *d = reinterpret_cast<uint4 *>(&dst);
+    for (int k = tid; k < (int)(sizeof(Packed) / 16); k += nthreads) d[k] = s[k];
+}
+
+// The network on the warp's 32 rows: lane l supplies its standardised input
+// row x (4 values) and receives its standardised output row y (3 values).
+// All 32 lanes of the warp must call it together; io is the warp's exchange
+// area.
+__device__ __forceinline__ void rows_forward(const Packed &P, float (*io)[4], int lane, const float x[4], float y[3])
+{
+    const int g = lane >> 2, tg = lane & 3;
+    io[lane][0] = x[0]; io[lane][1] = x[1]; io[lane][2] = x[2]; io[lane][3] = x[3];
+    __syncwarp();
+    float out[2][4];
+#pragma unroll
+    for (int mt = 0; mt < 2; mt++) {
+        const int r0 = mt * 16 + g, r1 = r0 + 8;
+        uint32_t ax[4];
+        ax[0] = tg < 2 ? pack_bf16x2(io[r0][2 * tg], io[r0][2 * tg + 1]) : 0u;
+        ax[1] = tg < 2 ? pack_bf16x2(io[r1][2 * tg], io[r1][2 * tg + 1]) : 0u;
+        ax[2] = 0u;
+        ax[3] = 0u;
+        // layer 1: [16 x 16] x [16 x 64] -> SiLU -> A fragments of layer 2
+        uint32_t a[4][4];
+#pragma unroll
+        for (int kt = 0; kt < 4; kt++) {
+            float c0[4], c1[4];
+            const int n0 = (2 * kt) * 8, n1 = n0 + 8;
+            c0[0] = P.b1[n0 + 2 * tg]; c0[1] = P.b1[n0 + 2 * tg + 1]; c0[2] = c0[0]; c0[3] = c0[1];
+            c1[0] = P.b1[n1 + 2 * tg]; c1[1] = P.b1[n1 + 2 * tg + 1]; c1[2] = c1[0]; c1[3] = c1[1];
+            mma_bf16_16816(c0, ax, P.w1[n0 + g][tg], P.w1[n0 + g][tg + 4]);
+            mma_bf16_16816(c1, ax, P.w1[n1 + g][tg], P.w1[n1 + g][tg + 4]);
+            a[kt][0] = pack_bf16x2(silu_fast(c0[0]), silu_fast(c0[1]));
+            a[kt][1] = pack_bf16x2(silu_fast(c0[2]), silu_fast(c0[3]));
+            a[kt][2] = pack_bf16x2(silu_fast(c1[0]), silu_fast(c1[1]));
+            a[kt][3] = pack_bf16x2(silu_fast(c1[2]), silu_fast(c1[3]));
+        }
+        // layer 2: [16 x 64] x [64 x 64] -> SiLU, two n-tiles at a time into
+        // the A fragment of layer 3 ([16 x 64] x [64 x 8])
+        float d[4] = {P.b3[2 * tg], P.b3[2 * tg + 1], P.b3[2 * tg], P.b3[2 * tg + 1]};
+#pragma unroll
+        for (int kt = 0; kt < 4; kt++) {
+            float c0[4], c1[4];
+            const int n0 = (2 * kt) * 8, n1 = n0 + 8;
+            c0[0] = P.b2[n0 + 2 * tg]; c0[1] = P.b2[n0 + 2 * tg + 1]; c0[2] = c0[0]; c0[3] = c0[1];
+            c1[0] = P.b2[n1 + 2 * tg]; c1[1] = P.b2[n1 + 2 * tg + 1]; c1[2] = c1[0]; c1[3] = c1[1];
+#pragma unroll
+            for (int k2 = 0; k2 < 4; k2++) {
+                mma_bf16_16816(c0, a[k2], P.w2[n0 + g][k2 * 8 + tg], P.w2[n0 + g][k2 * 8 + tg + 4]);
+                mma_bf16_16816(c1, a[k2], P.w2[n1 + g][k2 * 8 + tg], P.w2[n1 + g][k2 * 8 + tg + 4]);
+            }
+            uint32_t a2[4];
+            a2[0] = pack_bf16x2(silu_fast(c0[0]), silu_fast(c0[1]));
+            a2[1] = pack_bf16x2(silu_fast(c0[2]), silu_fast(c0[3]));
+            a2[2] = pack_bf16x2(silu_fast(c1[0]), silu_fast(c1[1]));
+            a2[3] = pack_bf16x2(silu_fast(c1[2]), silu_fast(c1[3]));
+            mma_bf16_16816(d, a2, P.w3[g][kt * 8 + tg], P.w3[g][kt * 8 + tg + 4]);
+        }
+        out[mt][0] = d[0]; out[mt][1] = d[1]; out[mt][2] = d[2]; out[mt][3] = d[3];
+    }
+    __syncwarp();
+    // columns 2tg, 2tg+1 of rows g and g+8 of each m-tile; outputs 0..2 are in lanes with tg < 2
+    if (tg < 2) {
+#pragma unroll
+        for (int mt = 0; mt < 2; mt++) {
+            io[mt * 16 + g][2 * tg] = out[mt][0];
+            io[mt * 16 + g][2 * tg + 1] = out[mt][1];
+            io[mt * 16 + g + 8][2 * tg] = out[mt][2];
+            io[mt * 16 + g + 8][2 * tg + 1] = out[mt][3];
+        }
+    }
+    __syncwarp();
+    y[0] = io[lane][0]; y[1] = io[lane][1]; y[2] = io[lane][2];
+    __syncwarp();
+}
+
+}  // namespace mlp
+}  // namespace icempm

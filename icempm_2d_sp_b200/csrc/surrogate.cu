@@ -36,13 +36,11 @@
 
 #include "engine.cuh"
 #include "engine_iface.h"
+#include "mlp_device.cuh"
 
 namespace icempm {
 namespace mlp {
 
-constexpr int IN = 4, HID = 64, OUT = 3;
-constexpr int W1 = 0, B1 = W1 + HID * IN, W2 = B1 + HID, B2 = W2 + HID * HID, W3 = B2 + HID, B3 = W3 + OUT * HID;
-constexpr int NPARAM = B3 + OUT;   // 4675
 constexpr int BLK = 128, LD = HID + 1;
 
 __device__ __forceinline__ float sigm(float z) { return 1.0f / (1.0f + expf(-z)); }
@@ -391,7 +389,41 @@ __global__ void __launch_bounds__(IWARPS * 32) k_return_map_learned(MatT<float> 
     }
 }
 
+// FP32 master parameters and normalisation -> the packed network
+// (mlp_device.cuh), one thread per word.
+__global__ void k_mlp_pack(const float *__restrict__ P, const float *__restrict__ norm, Packed *out)
+{
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < HID * 8) {                       // w1: k 2c, 2c+1 of row n (k >= IN is padding)
+        const int n = e / 8, c = e % 8, k = 2 * c;
+        out->w1[n][c] = pack_bf16x2(k < IN ? P[W1 + n * IN + k] : 0.0f, k + 1 < IN ? P[W1 + n * IN + k + 1] : 0.0f);
+    }
+    if (e < HID * HID / 2) {
+        const int n = e / (HID / 2), c = e % (HID / 2);
+        out->w2[n][c] = pack_bf16x2(P[W2 + n * HID + 2 * c], P[W2 + n * HID + 2 * c + 1]);
+    }
+    if (e < 8 * HID / 2) {                   // w3: rows n >= OUT are padding
+        const int n = e / (HID / 2), c = e % (HID / 2);
+        out->w3[n][c] = n < OUT ? pack_bf16x2(P[W3 + n * HID + 2 * c], P[W3 + n * HID + 2 * c + 1]) : 0u;
+    }
+    if (e < HID) { out->b1[e] = P[B1 + e]; out->b2[e] = P[B2 + e]; }
+    if (e < 8) out->b3[e] = e < OUT ? P[B3 + e] : 0.0f;
+    if (e < 16) out->norm[e] = e < 14 ? norm[e] : 0.0f;
+}
+
 }  // namespace mlp
+
+int mlp_pack(const float *d_params, const float *d_norm, void *d_packed, cudaStream_t stream)
+{
+    mlp::k_mlp_pack<<<(mlp::HID * mlp::HID / 2 + 255) / 256, 256, 0, stream>>>(d_params, d_norm,
+                                                                             (mlp::Packed *)d_packed);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(ICEMPM_E_CUDA, std::string("k_mlp_pack: ") + cudaGetErrorString(e));
+    return ICEMPM_OK;
+}
+
+size_t mlp_packed_bytes() { return sizeof(mlp::Packed); }
+
 }  // namespace icempm
 
 using icempm::fail;

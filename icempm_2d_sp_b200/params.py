@@ -37,8 +37,8 @@ ERR_GRID_NAN = 0x0400
 ERR_FIXED_OVERFLOW = 0x1000
 ERR_BARRIER_TIMEOUT = 0x2000
 
-VARIANT_FIXED, VARIANT_FP32, VARIANT_FP64 = 0, 1, 2
-VARIANTS = {"fixed": VARIANT_FIXED, "fp32": VARIANT_FP32, "fp64": VARIANT_FP64}
+VARIANT_FIXED, VARIANT_FP32, VARIANT_FP64, VARIANT_TEXTBOOK = 0, 1, 2, 3
+VARIANTS = {"fixed": VARIANT_FIXED, "fp32": VARIANT_FP32, "fp64": VARIANT_FP64, "textbook": VARIANT_TEXTBOOK}
 FORCING_COMPAT, FORCING_EXTENDED = 0, 1
 WIND_NONE, WIND_UNIFORM, WIND_RANKINE = 0, 1, 2
 

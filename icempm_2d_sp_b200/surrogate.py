@@ -181,3 +181,34 @@ def learned_map(prms, params, norm, trial, tol=1e-4, repeat=1):
     e1.record()
     torch.cuda.synchronize()
     return od.cpu().numpy(), nfb, e0.elapsed_time(e1) / repeat
+
+
+def train(records, epochs=30, batch=1024, lr=3e-3, seed=0):
+    """Standardisation and network fitted to harvested records [n, 8]
+    (trial 0..3, projected 4..6); returns (params, Norm, loss history)."""
+    x = feats(records[:, :4])
+    y = targets(records[:, :4], records[:, 4:7])
+    norm = Norm.fit(x, y)
+    xs = ((x - norm.x_mean) / norm.x_std).astype(np.float32)
+    ys = ((y - norm.y_mean) / norm.y_std).astype(np.float32)
+    tr = Trainer(lr=lr, seed=seed)
+    hist = tr.fit(xs, ys, epochs=epochs, batch=batch, seed=seed)
+    return tr.params(), norm, hist
+
+
+class StepNetwork:
+    """A trained network on the device for a context's step path
+    (Context.set_learned_map): holds the FP32 parameters and the
+    normalisation in device memory for as long as the context uses them."""
+
+    def __init__(self, params, norm: Norm):
+        import torch
+        self.P = torch.from_numpy(np.asarray(params, np.float32).copy()).cuda()
+        self.N = torch.from_numpy(norm.vector()).cuda()
+
+    def attach(self, ctx, tol):
+        ctx.set_learned_map(C.c_void_p(self.P.data_ptr()), C.c_void_p(self.N.data_ptr()), tol)
+
+    @staticmethod
+    def detach(ctx):
+        ctx.set_learned_map(None, None, 1.0)

@@ -135,7 +135,10 @@ enum {
 enum {
     ICEMPM_VARIANT_FIXED = 0, /* FP32 state, int64 fixed-point P2G (deterministic) */
     ICEMPM_VARIANT_FP32  = 1, /* FP32 state, FP32 atomics                           */
-    ICEMPM_VARIANT_FP64  = 2  /* FP64 state and arithmetic, FP64 atomics            */
+    ICEMPM_VARIANT_FP64  = 2, /* FP64 state and arithmetic, FP64 atomics            */
+    ICEMPM_VARIANT_TEXTBOOK = 3 /* the plain FP32 baseline: three unfused kernels, one point or
+                                   node per thread, 27 global FP32 atomics per point in P2G
+                                   (for comparison; never faster) */
 };
 enum {
     ICEMPM_FORCING_COMPAT   = 0, /* reference grid update: effective drag + current ramp (kernels.cuh:141-169) */
@@ -278,6 +281,15 @@ ICEMPM_API int icempm_get_boundary_forces(icempm_t *ctx, double *fxfy, int32_t e
  * re-upload (host_side_soa.cpp:36-47, model.cpp:63-72); ties keep their
  * previous relative order.  Resets the disabled counter to 0. */
 ICEMPM_API int icempm_sort_compact(icempm_t *ctx);
+
+/* Sort cadence from a measurement on the live scene (no reference
+ * counterpart: the reference re-sorts only when it compacts, host_side_soa.cpp:36-47).
+ * Advances the scene 2 * trial_steps sub-steps from first_step: trial_steps in
+ * the current point order, one locality sort (timed), trial_steps in the
+ * sorted order.  Cadence k in {100, 400} is kept when the sorted order's
+ * ms/step plus the sort's ms / k beats the current order's ms/step, else 0;
+ * the choice becomes the context's sort_every and is returned. */
+ICEMPM_API int icempm_tune_sort_cadence(icempm_t *ctx, int32_t trial_steps, int32_t first_step, int32_t *sort_every);
 
 /* Device time of the last icempm_step call, in ms: [0] total, [1] grid
  * update kernels, [2] fused G2P+P2G kernels, [3] locality re-sorts.
@@ -432,6 +444,19 @@ ICEMPM_API int icempm_return_map_exact(const icempm_simparams_t *prms, const flo
 ICEMPM_API int icempm_return_map_learned(const icempm_simparams_t *prms, const float *d_params, const float *d_norm,
                                          const float *d_trial, uint32_t n, float tol, float *d_out,
                                          uint32_t *d_fallbacks, void *stream);
+/* The learned map on the step path: from now on the fused kernel sends every
+ * crushed point's projection onto the yield surface (wolper_dp case 3,
+ * kernels.cuh:400-467, as called from partition_kernel_g2p, kernels.cuh:271-283)
+ * to the network, evaluated in place by BF16 tensor-core MMAs with FP32
+ * accumulation over the warp's points; an answer off the yield surface by
+ * more than tol (as icempm_return_map_learned) is replaced by the exact map.
+ * d_params (ICEMPM mlp parameters) and d_norm (14 floats) are device
+ * pointers, packed at the call; d_params NULL switches the network off.
+ * FP32-state variants only.  Resets the counts below. */
+ICEMPM_API int icempm_set_learned_map(icempm_t *ctx, const float *d_params, const float *d_norm, float tol);
+/* Projections the network answered (*kept) and those that fell back to the
+ * exact map (*fallbacks) since icempm_set_learned_map.  Synchronises. */
+ICEMPM_API int icempm_learned_map_counts(icempm_t *ctx, uint64_t *kept, uint64_t *fallbacks);
 /* Training data from a run: from now on the fused kernel records up to
  * `capacity` projections (trial, projected) of crushed points with
  * (index + sub-step) % stride == 0.  icempm_harvest_end copies the records

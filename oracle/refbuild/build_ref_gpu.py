@@ -22,7 +22,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE = os.path.dirname(HERE)
 OUT_DIR = os.path.join(ORACLE, "_ref")
 LIB = os.path.join(OUT_DIR, "libicempm_ref_gpu.so")
-REF = os.environ.get("ICEMPM_REFERENCE_DIR", "/root/reference")
+# the reference checkout: ICEMPM_REFERENCE_DIR, else the one build_ref.py uses
+from oracle.refbuild.build_ref import REF  # noqa: E402
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 

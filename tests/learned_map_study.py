@@ -1,8 +1,9 @@
 """Learned return map study (16M-point ridging scene, 8192x2048 grid).
 
 1. Training pairs: projections recorded by the fused kernel from plain-method
-   runs -- the 1M-point ridging scene (1024x512 grid, 2 m/s against the wall)
-   and the floe-field scene on a 2048x1024 grid -- up to --pairs records.
+   runs -- the floe-field scene (config-1 rules on a 2048x1024 grid, 200
+   sub-steps) and 1M-point ridging scenes (1024x512 grid, against the wall at
+   1-4 m/s, 1000 sub-steps each) -- up to --pairs records.
 2. Training: the library's GPU kernels (icempm_mlp_grad + icempm_mlp_adam),
    minibatch Adam on standardised features.
 3. Evaluation: trial states recorded from a 16M-point compressive ridging
@@ -10,6 +11,9 @@
    sub-steps), mapped by the learned map (BF16 tensor cores, exact fallback
    above the yield residual) and by the exact map (FP32 and FP64): fallback
    rate, error of the answers against FP64, device time per trial state.
+4. The learned map fused into the step (icempm_set_learned_map) on the same
+   scene and sub-steps against the exact step: device time per sub-step,
+   answers kept and fallbacks, state deviation from the FP64 variant.
 
     python tests/learned_map_study.py [--pairs 20000000] [--eval-steps 500] [--json out.json]
 
@@ -43,6 +47,46 @@ def harvest(sc, steps, capacity, stride, forcing_opts=True):
     return rec, offered
 
 
+def run_scene(sc, steps, variant="fixed", net=None, tol=None):
+    """The scene advanced `steps` sub-steps (CUDA graphs); returns (state,
+    error bits, device ms per sub-step, (kept, fallbacks))."""
+    with capi.Context(sc.prms, sc.status, sc.current, capacity=sc.n,
+                      options=Options.default(variant=variant, forcing=sc.options.forcing)) as ctx:
+        ctx.upload(sc.soa, sc.n)
+        if net is not None:
+            net.attach(ctx, tol)
+        ctx.step(steps, 0)
+        ms = ctx.timings()[0] / steps
+        out, _ = ctx.download(np.zeros_like(sc.soa))
+        err, _ = ctx.status()
+        counts = ctx.learned_map_counts() if net is not None else (0, 0)
+    return out, err, ms, counts
+
+
+def fused_runs(sc, params, norm, steps):
+    n = sc.n
+    ref64, e64, ms64, _ = run_scene(sc, steps, "fp64")
+    vref = np.abs(ref64[8:10, :n]).max()
+
+    def dev(st):
+        return {"pos_max_cells": float(np.abs(st[6:8, :n] - ref64[6:8, :n]).max()),
+                "vel_max_rel": float(np.abs(st[8:10, :n] - ref64[8:10, :n]).max() / vref),
+                "vel_rms_rel": float(np.sqrt(((st[8:10, :n] - ref64[8:10, :n]) ** 2).mean()) / vref),
+                "fe_max": float(np.abs(st[10:14, :n] - ref64[10:14, :n]).max()),
+                "jp_max_rel": float(np.abs(st[5, :n] / ref64[5, :n] - 1.0).max())}
+    exact, e0, ms0, _ = run_scene(sc, steps)
+    res = {"points": int(n), "steps": steps, "fp64_ms_per_step": ms64,
+           "exact": {"ms_per_step": ms0, "err_bits": int(e0), **dev(exact)}}
+    net = surrogate.StepNetwork(params, norm)
+    for tol in (1e-4, 1e-3, 1e-2):
+        st, e1, ms1, (kept, fb) = run_scene(sc, steps, net=net, tol=tol)
+        res["learned_tol_%g" % tol] = {"ms_per_step": ms1, "err_bits": int(e1), "kept": int(kept),
+                                       "fallback": int(fb), "fallback_rate": fb / max(1, kept + fb), **dev(st)}
+        print(f"# fused learned map tol {tol}: {ms1:.4f} ms/step (exact {ms0:.4f}), kept {kept}, fallback {fb}",
+              file=sys.stderr)
+    return res
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--pairs", type=int, default=20_000_000)
@@ -53,17 +97,23 @@ def main():
     a = ap.parse_args()
     out = {}
     t0 = time.time()
-    # 1. training pairs
-    r1, o1 = harvest(scenes.ridging(), 1000, a.pairs, 2)
-    parts = [r1]
-    if len(r1) < a.pairs:
-        sc1 = scenes.floe_field(gx=2048, gy=1024, n_seeds=500)
-        r2, o2 = harvest(sc1, 200, a.pairs - len(r1), 1)
-        parts.append(r2)
-        out["pairs_floe_field"] = int(len(r2))
+    # 1. training pairs: the floe-field scene (config-1 rules on a 2048x1024
+    # grid, 200 sub-steps), then ridging runs at several speeds until --pairs
+    sc1 = scenes.floe_field(gx=2048, gy=1024, n_seeds=500)
+    r0, _ = harvest(sc1, 200, a.pairs, 1)
+    out["pairs_floe_field"] = int(len(r0))
+    parts = [r0]
+    have = len(r0)
+    out["pairs_ridging"] = []
+    for seed, speed in ((1236, 2.0), (1237, 1.0), (1238, 4.0), (1239, 3.0), (1240, 1.5), (1241, 2.5)):
+        if have >= a.pairs:
+            break
+        r1, _ = harvest(scenes.ridging(seed=seed, speed=speed), 1000, a.pairs - have, 1)
+        parts.append(r1)
+        have += len(r1)
+        out["pairs_ridging"].append({"seed": seed, "speed": speed, "pairs": int(len(r1))})
     rec = np.concatenate(parts)
     out["pairs"] = int(len(rec))
-    out["pairs_ridging"] = int(len(r1))
     print(f"# {len(rec)} pairs ({time.time() - t0:.1f} s)", file=sys.stderr)
     # 2. training
     x = surrogate.feats(rec[:, :4])
@@ -105,6 +155,10 @@ def main():
     raw, _, ms_raw = surrogate.learned_map(ev.prms, params, norm, trial[:, :4], tol=1e30, repeat=5)
     er = rel(raw, exact64)
     out["network_only"] = {"ms": ms_raw, "err_max": float(er.max()), "err_rms": float(np.sqrt((er ** 2).mean()))}
+    # 4. the learned map fused into the step (icempm_set_learned_map) against
+    # the exact step on the same scene and sub-steps; error against the FP64
+    # variant's state
+    out["fused"] = fused_runs(ev, params, norm, a.eval_steps)
     print(json.dumps(out, indent=1))
     if a.json:
         with open(a.json, "w") as f:

@@ -61,7 +61,7 @@ def run_gpu(capi, prms, status, current, soa_in, n, nsteps, first_step, variant,
     return out, err, dis
 
 
-@pytest.mark.parametrize("variant", ["fixed", "fp32", "fp64"])
+@pytest.mark.parametrize("variant", ["fixed", "fp32", "fp64", "textbook"])
 def test_one_step_golden(capi, variant):
     z, prms = load_fixture("random_1step")
     n = int(z["n"])
@@ -82,7 +82,7 @@ def test_one_step_golden(capi, variant):
 MULTI = ["random_10step", "random_plastic_20step", "ridging_60step", "disable_then_sort"]
 
 
-@pytest.mark.parametrize("variant", ["fixed", "fp32", "fp64"])
+@pytest.mark.parametrize("variant", ["fixed", "fp32", "fp64", "textbook"])
 @pytest.mark.parametrize("name", MULTI)
 def test_multi_step_golden(capi, name, variant):
     z, prms = load_fixture(name)

@@ -43,6 +43,63 @@ def harvested(capi):
     return sc, rec, offered
 
 
+@pytest.fixture(scope="module")
+def trained(capi, harvested):
+    """A network fitted to the harvested projections (30 epochs)."""
+    _, rec, _ = harvested
+    params, norm, hist = surrogate.train(rec, epochs=30)
+    assert hist[-1] < 0.25 * hist[0], hist
+    return params, norm
+
+
+def _run(capi, sc, steps, net=None, tol=None):
+    """The scene advanced `steps` sub-steps with the exact map or, with a
+    network, the fused learned map; returns (state, error bits, device ms per
+    sub-step, (kept, fallbacks))."""
+    with capi.Context(sc.prms, sc.status, sc.current, capacity=sc.n,
+                      options=Options.default(use_graphs=0)) as ctx:
+        ctx.upload(sc.soa, sc.n)
+        if net is not None:
+            net.attach(ctx, tol)
+        ctx.step(steps, 0)
+        ms = ctx.timings()[0] / steps
+        out, _ = ctx.download(np.zeros_like(sc.soa))
+        err, _ = ctx.status()
+        counts = ctx.learned_map_counts() if net is not None else (0, 0)
+    return out, err, ms, counts
+
+
+def test_learned_map_fused_into_the_step(capi, harvested, trained):
+    """The learned map on the step path (icempm_set_learned_map): the fused
+    kernel sends its case-3 projections to the network.  With a tolerance no
+    answer meets, every projection falls back to the exact map and the state
+    equals the exact step's (the parity tests' FP32 tolerances for 10-60
+    steps: positions 1e-4 cells, velocities 1e-3 relative, |dFe| 1e-5); with a loose tolerance
+    the network's answers are kept and the run stays finite and error-free.
+    The device times of both forms are measured beside each other."""
+    sc, _, _ = harvested
+    params, norm = trained
+    net = surrogate.StepNetwork(params, norm)
+    steps = 40
+    ref, err0, ms_exact, _ = _run(capi, sc, steps)
+    tight, err1, ms_tight, (kept1, fb1) = _run(capi, sc, steps, net, 1e-30)
+    assert err0 == 0 and err1 == 0
+    assert kept1 == 0 and fb1 > 1000
+    n = sc.n
+    vref = np.abs(ref[8:10, :n]).max()
+    assert np.abs(tight[6:8, :n] - ref[6:8, :n]).max() <= 1e-4
+    assert np.abs(tight[8:10, :n] - ref[8:10, :n]).max() <= 1e-3 * vref
+    assert np.abs(tight[10:14, :n] - ref[10:14, :n]).max() <= 1e-5
+    loose, err2, ms_loose, (kept2, fb2) = _run(capi, sc, steps, net, 1e-2)
+    assert err2 == 0 and kept2 > 0
+    assert np.all(np.isfinite(loose[6:18, :n]))
+    dv = np.abs(loose[8:10, :n] - ref[8:10, :n]).max() / vref
+    print(f"\nfused learned map, {steps} sub-steps of {n} points: exact {ms_exact:.4f} ms/step; "
+          f"network with every answer rejected {ms_tight:.4f} ms/step; tol 1e-2: {ms_loose:.4f} ms/step, "
+          f"kept {kept2}, fallback {fb2}, max velocity deviation {dv:.2e}")
+    assert ms_exact > 0 and ms_tight > 0 and ms_loose > 0
+
+
 def test_mlp_gradients_match_fp64_reference(capi):
     from oracle import mlp_reference as ref
     import torch

@@ -105,13 +105,17 @@ def main():
     parts = [r0]
     have = len(r0)
     out["pairs_ridging"] = []
-    for seed, speed in ((1236, 2.0), (1237, 1.0), (1238, 4.0), (1239, 3.0), (1240, 1.5), (1241, 2.5)):
+    # four ridging runs share the pairs; every 4th point-step is offered, so a
+    # run's records spread over its 1000 sub-steps instead of its first ones
+    runs = ((1236, 2.0), (1237, 1.0), (1238, 4.0), (1239, 3.0))
+    for k, (seed, speed) in enumerate(runs):
         if have >= a.pairs:
             break
-        r1, _ = harvest(scenes.ridging(seed=seed, speed=speed), 1000, a.pairs - have, 1)
+        cap = -(-(a.pairs - have) // (len(runs) - k))
+        r1, offered = harvest(scenes.ridging(seed=seed, speed=speed), 1000, cap, 4)
         parts.append(r1)
         have += len(r1)
-        out["pairs_ridging"].append({"seed": seed, "speed": speed, "pairs": int(len(r1))})
+        out["pairs_ridging"].append({"seed": seed, "speed": speed, "pairs": int(len(r1)), "offered": int(offered)})
     rec = np.concatenate(parts)
     out["pairs"] = int(len(rec))
     print(f"# {len(rec)} pairs ({time.time() - t0:.1f} s)", file=sys.stderr)

@@ -1441,7 +1441,7 @@ __device__ __forceinline__ void fused_chunk(ChunkSmem<Real, Acc, BT, PPT, CAP, S
     // ---- phase 2 ----------------------------------------------------------
     Patch<Real> patch;
     patch.have = false; patch.in_tile = false; patch.cx = patch.cy = 0;
-#pragma unroll 1
+#pragma unroll
     for (int j = 0; j < PPT; j++) {
         const int local = wbase + 32 * j;
         if (base + (uint32_t)local >= (uint32_t)n) break;

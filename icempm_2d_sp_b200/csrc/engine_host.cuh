@@ -801,13 +801,13 @@ public:
     {
         if (elapsed <= 0) return fail(ICEMPM_E_ARG, "elapsed_steps must be > 0");
         if (!frame_mem_) {
-            const size_t bytes = G_ * (kFrameChannels * sizeof(float) + sizeof(uint32_t) + 5) +
+            const size_t bytes = G_ * (3 * sizeof(float4) + kFrameChannels * sizeof(float) + 5) +
                                  2 * ICEMPM_MAX_REGIONS * sizeof(float) + 256;
             ICEMPM_CUDA(cudaMalloc(&frame_mem_, bytes));
             char *b = (char *)frame_mem_;
-            for (int c = 0; c < kFrameChannels; c++) { frame_.ch[c] = (float *)b; b += G_ * sizeof(float); }
-            frame_.count = (uint32_t *)b; b += G_ * sizeof(uint32_t);
+            frame_.acc = (float4 *)b; b += G_ * 3 * sizeof(float4);
             frame_.region_force = (float *)b; b += 2 * ICEMPM_MAX_REGIONS * sizeof(float);
+            for (int c = 0; c < kFrameChannels; c++) { frame_.ch[c] = (float *)b; b += G_ * sizeof(float); }
             frame_.rgb = (uint8_t *)b; b += 3 * G_;
             frame_.mask = (uint8_t *)b; b += G_;
             frame_.count8 = (uint8_t *)b;
@@ -822,8 +822,7 @@ public:
             ICEMPM_CUDA(cudaMemcpyAsync(colors_, colors, (size_t)ncolors * sizeof(uint32_t), cudaMemcpyHostToDevice,
                                         stream_));
         }
-        const size_t zero_bytes = G_ * (kFrameChannels * sizeof(float) + sizeof(uint32_t)) +
-                                  2 * ICEMPM_MAX_REGIONS * sizeof(float);
+        const size_t zero_bytes = G_ * 3 * sizeof(float4) + 2 * ICEMPM_MAX_REGIONS * sizeof(float);
         ICEMPM_CUDA(cudaMemsetAsync(frame_mem_, 0, zero_bytes, stream_));
         if (n_ > 0) {
             k_frame_scatter<Real><<<(n_ + 1023) / 1024, 256, 0, stream_>>>(

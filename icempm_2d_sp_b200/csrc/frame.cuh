@@ -12,9 +12,11 @@
 // (status >= 100 -> status - 99, else status).
 //
 // k_frame_scatter: four entries of the locality order per thread (one cell,
-// as the sort arranged them), summed in registers per node; a CTA's nodes are
-// accumulated in a shared tile (FP32 shared atomics) and flushed with one
-// global atomic per non-zero node and channel.
+// as the sort arranged them), their node terms summed in registers node by
+// node; each node's sums go straight to the global accumulators with three
+// 16-byte vector reductions (`red.global.add.v4.f32`): a node's eleven
+// channels (the ten above and the point count of its cell) are interleaved
+// in three float4.
 // k_frame_finish: one node per thread; region sums reduced in shared memory.
 #pragma once
 #include "engine.cuh"
@@ -22,13 +24,12 @@
 namespace icempm {
 
 constexpr int kFrameChannels = 10;   // density, mass, m vx, m vy, Jp_inv, P, Q, r, g, b
-constexpr int kFrameTile = 1024;     // nodes of a CTA's shared tile
 // water colour (ColorMap::rgb_water, gui/colormap.h:36)
 __host__ __device__ constexpr float water_rgb(int k) { return k == 0 ? 21.0f : (k == 1 ? 31.0f : 47.0f); }
 
 struct FrameOut {
-    float *ch[kFrameChannels];   // G each: the accumulated, then finished channels
-    uint32_t *count;             // G: points per cell (the reference keeps the low 8 bits)
+    float4 *acc;                 // 3 per node: the ten channels and the cell's point count, interleaved
+    float *ch[kFrameChannels];   // G each: the finished channels
     uint8_t *rgb, *mask, *count8;
     float *region_force;         // 2 * ICEMPM_MAX_REGIONS
 };
@@ -50,41 +51,37 @@ __device__ __forceinline__ void frame_values(const Pts<Real> &P, int i, Real par
     x = float(A.x); y = float(A.y);
 }
 
-// Adds node (X, Y)'s channel sums into the CTA tile, or into the grid when
-// the tile is off.
-__device__ __forceinline__ void frame_node_add(float (*tile)[kFrameTile], bool on, int x0, int y0, int th,
-                                               const FrameOut &F, int gy, int X, int Y, const float add[kFrameChannels])
+__device__ __forceinline__ void red_add_v4(float4 *a, float x, float y, float z, float w)
 {
-    if (on) {
-        const int li = (X - x0) * th + (Y - y0);
-#pragma unroll
-        for (int c = 0; c < kFrameChannels; c++) atomicAdd(&tile[c][li], add[c]);
-    } else {
-        const size_t node = (size_t)X * gy + Y;
-#pragma unroll
-        for (int c = 0; c < kFrameChannels; c++) atomicAdd(&F.ch[c][node], add[c]);
-    }
+    asm volatile("red.relaxed.gpu.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(a), "f"(x), "f"(y), "f"(z),
+                 "f"(w)
+                 : "memory");
+}
+
+// Adds node (X, Y)'s channel sums and `count` points to the accumulators.
+__device__ __forceinline__ void frame_node_add(const FrameOut &F, int gy, int X, int Y, const float add[kFrameChannels],
+                                               float count)
+{
+    float4 *a = F.acc + 3 * ((size_t)X * gy + Y);
+    red_add_v4(a, add[0], add[1], add[2], add[3]);
+    red_add_v4(a + 1, add[4], add[5], add[6], add[7]);
+    red_add_v4(a + 2, add[8], add[9], count, 0.0f);
 }
 
 // A CTA takes 1024 entries of the locality order: 8 warps x 128, thread
 // (warp w, lane l) the entries w*128 + 32j + l, j = 0..3, which the sort put
 // in one cell.  When a thread's enabled points do share a cell, their node
-// terms are summed in registers first (one shared atomic per node and
-// channel for up to four points); otherwise each point adds its own.
+// terms are summed in registers first (three reductions per node for up to
+// four points); otherwise each point adds its own.
 template <class Real>
 __global__ void __launch_bounds__(256) k_frame_scatter(Pts<Real> P, int n, int gx, int gy, Real particle_mass,
                                                        const uint32_t *__restrict__ colors, uint32_t ncolors,
                                                        FrameOut F)
 {
-    __shared__ float tile[kFrameChannels][kFrameTile];
-    __shared__ int box[4];
-    if (threadIdx.x == 0) { box[0] = INT_MAX; box[1] = INT_MAX; box[2] = -1; box[3] = -1; }
-    __syncthreads();
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int e0 = blockIdx.x * 1024 + w * 128 + lane;
     bool act[4];
     int cxs[4], cys[4];
-    unsigned xmn = 0x7fffffffu, ymn = 0x7fffffffu, xmx = 0u, ymx = 0u;
 #pragma unroll
     for (int j = 0; j < 4; j++) {
         const int i = e0 + 32 * j;
@@ -94,33 +91,8 @@ __global__ void __launch_bounds__(256) k_frame_scatter(Pts<Real> P, int n, int g
             const int cx = (int)(key.x & 0xffff), cy = (int)(key.x >> 16);
             act[j] = !(key.y & kDisabled) && cx >= 1 && cx <= gx - 2 && cy >= 1 && cy <= gy - 2;
             cxs[j] = cx; cys[j] = cy;
-            if (act[j]) {
-                xmn = min(xmn, (unsigned)cx); ymn = min(ymn, (unsigned)cy);
-                xmx = max(xmx, (unsigned)cx); ymx = max(ymx, (unsigned)cy);
-            }
         }
     }
-    {
-        const unsigned FULL = 0xffffffffu;
-        xmn = __reduce_min_sync(FULL, xmn); ymn = __reduce_min_sync(FULL, ymn);
-        xmx = __reduce_max_sync(FULL, xmx); ymx = __reduce_max_sync(FULL, ymx);
-        const bool any = act[0] || act[1] || act[2] || act[3];
-        const bool warp_any = __any_sync(FULL, any);   // every lane votes (a skipped lane stalls the warp)
-        if (lane == 0 && warp_any) {
-            atomicMin(&box[0], (int)xmn); atomicMin(&box[1], (int)ymn);
-            atomicMax(&box[2], (int)xmx); atomicMax(&box[3], (int)ymx);
-        }
-    }
-    __syncthreads();
-    const int x0 = box[0] - 1, y0 = box[1] - 1;
-    const int tw = box[2] - box[0] + 3, th = box[3] - box[1] + 3;
-    const bool on = box[2] >= 0 && (long long)tw * (long long)th <= (long long)kFrameTile;
-    const int nt = on ? tw * th : 0;
-    for (int k = threadIdx.x; k < nt; k += 256)
-#pragma unroll
-        for (int c = 0; c < kFrameChannels; c++) tile[c][k] = 0.0f;
-    __syncthreads();
-
     // the thread's enabled points: one cell?
     int first = -1, nact = 0;
     bool one_cell = true;
@@ -161,9 +133,8 @@ __global__ void __launch_bounds__(256) k_frame_scatter(Pts<Real> P, int n, int g
 #pragma unroll
                     for (int c = 0; c < kFrameChannels; c++) add[c] += wgt * vals[j][c];
                 }
-                frame_node_add(tile, on, x0, y0, th, F, gy, cx + a - 1, cy + b - 1, add);
+                frame_node_add(F, gy, cx + a - 1, cy + b - 1, add, (a == 1 && b == 1) ? float(nact) : 0.0f);
             }
-        atomicAdd(&F.count[(size_t)cx * gy + cy], (uint32_t)nact);
     } else if (nact > 0) {
 #pragma unroll 1
         for (int j = 0; j < 4; j++) {
@@ -178,18 +149,9 @@ __global__ void __launch_bounds__(256) k_frame_scatter(Pts<Real> P, int n, int g
                     float add[kFrameChannels];
 #pragma unroll
                     for (int c = 0; c < kFrameChannels; c++) add[c] = wgt * vals[c];
-                    frame_node_add(tile, on, x0, y0, th, F, gy, cxs[j] + a - 1, cys[j] + b - 1, add);
+                    frame_node_add(F, gy, cxs[j] + a - 1, cys[j] + b - 1, add, (a == 1 && b == 1) ? 1.0f : 0.0f);
                 }
-            atomicAdd(&F.count[(size_t)cxs[j] * gy + cys[j]], 1u);
         }
-    }
-    __syncthreads();
-    for (int k = threadIdx.x; k < nt; k += 256) {
-        const int lx = k / th, ly = k - lx * th;
-        const size_t node = (size_t)(x0 + lx) * gy + (y0 + ly);
-#pragma unroll
-        for (int c = 0; c < kFrameChannels; c++)
-            if (tile[c][k] != 0.0f) atomicAdd(&F.ch[c][node], tile[c][k]);
     }
 }
 
@@ -204,9 +166,8 @@ static __global__ void __launch_bounds__(256) k_frame_finish(FrameOut F, const u
     __syncthreads();
     const long long i = (long long)blockIdx.x * 256 + threadIdx.x;
     if (i < G) {
-        float c[kFrameChannels];
-#pragma unroll
-        for (int k = 0; k < kFrameChannels; k++) c[k] = F.ch[k][i];
+        const float4 a0 = F.acc[3 * i], a1 = F.acc[3 * i + 1], a2 = F.acc[3 * i + 2];
+        float c[kFrameChannels] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w, a2.x, a2.y};
         const float density = c[0], mass = c[1];
         if (density > 0.0f) {
             const float coeff = 1.0f / density;
@@ -229,7 +190,7 @@ static __global__ void __launch_bounds__(256) k_frame_finish(FrameOut F, const u
 #pragma unroll
         for (int k = 0; k < kFrameChannels; k++) F.ch[k][i] = c[k];
         F.mask[i] = mask;
-        F.count8[i] = (uint8_t)F.count[i];
+        F.count8[i] = (uint8_t)(uint32_t)a2.z;   // the reference keeps the low 8 bits
         const int region = st >= 100 ? st - 99 : st;
         if (region < ICEMPM_MAX_REGIONS) {
             const double2 f = force[i];

@@ -51,13 +51,37 @@ __device__ __forceinline__ void mma_bf16_16816(float (&d)[4], const uint32_t (&a
                  : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
 
-// SiLU z sigmoid(z) = z/2 (1 + tanh(z/2)), with the hardware tanh
-// approximation (relative error ~2^-11, below the BF16 rounding that follows).
-__device__ __forceinline__ float silu_fast(float z)
+// One entry e of the packing of FP32 master parameters P and the
+// normalisation into a Packed network (entries 0 .. PACK_ENTRIES-1; every
+// word of the result is written by exactly one entry).
+constexpr int PACK_ENTRIES = HID * HID / 2;
+__device__ __forceinline__ void pack_entry(int e, const float *__restrict__ P, const float *__restrict__ norm,
+                                           Packed &out)
 {
-    float t;
-    asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(0.5f * z));
-    return 0.5f * z * (1.0f + t);
+    if (e < HID * 8) {                       // w1: k 2c, 2c+1 of row n (k >= IN is padding)
+        const int n = e / 8, c = e % 8, k = 2 * c;
+        out.w1[n][c] = pack_bf16x2(k < IN ? P[W1 + n * IN + k] : 0.0f, k + 1 < IN ? P[W1 + n * IN + k + 1] : 0.0f);
+    }
+    {
+        const int n = e / (HID / 2), c = e % (HID / 2);
+        out.w2[n][c] = pack_bf16x2(P[W2 + n * HID + 2 * c], P[W2 + n * HID + 2 * c + 1]);
+    }
+    if (e < 8 * HID / 2) {                   // w3: rows n >= OUT are padding
+        const int n = e / (HID / 2), c = e % (HID / 2);
+        out.w3[n][c] = n < OUT ? pack_bf16x2(P[W3 + n * HID + 2 * c], P[W3 + n * HID + 2 * c + 1]) : 0u;
+    }
+    if (e < HID) { out.b1[e] = P[B1 + e]; out.b2[e] = P[B2 + e]; }
+    if (e < 8) out.b3[e] = e < OUT ? P[B3 + e] : 0.0f;
+    if (e < 16) out.norm[e] = e < 14 ? norm[e] : 0.0f;
+}
+
+// SiLU z / (1 + exp(-z)) of two accumulator values with the fast exponential
+// and division intrinsics (a few ulp; the network is trained with the exact
+// form, and the hardware tanh approximation's ~2^-11 error measurably raised
+// the fallback rate), packed to a BF16 pair, the next layer's A-fragment word.
+__device__ __forceinline__ uint32_t silu_pack(float z0, float z1)
+{
+    return pack_bf16x2(__fdividef(z0, 1.0f + __expf(-z0)), __fdividef(z1, 1.0f + __expf(-z1)));
 }
 
 // Copies the packed network into shared memory (all threads of the CTA; a
@@ -78,8 +102,7 @@ __device__ __forceinline__ void rows_forward(const Packed &P, float (*io)[4], in
     const int g = lane >> 2, tg = lane & 3;
     io[lane][0] = x[0]; io[lane][1] = x[1]; io[lane][2] = x[2]; io[lane][3] = x[3];
     __syncwarp();
-    float out[2][4];
-#pragma unroll
+#pragma unroll 1
     for (int mt = 0; mt < 2; mt++) {
         const int r0 = mt * 16 + g, r1 = r0 + 8;
         uint32_t ax[4];
@@ -97,10 +120,10 @@ __device__ __forceinline__ void rows_forward(const Packed &P, float (*io)[4], in
             c1[0] = P.b1[n1 + 2 * tg]; c1[1] = P.b1[n1 + 2 * tg + 1]; c1[2] = c1[0]; c1[3] = c1[1];
             mma_bf16_16816(c0, ax, P.w1[n0 + g][tg], P.w1[n0 + g][tg + 4]);
             mma_bf16_16816(c1, ax, P.w1[n1 + g][tg], P.w1[n1 + g][tg + 4]);
-            a[kt][0] = pack_bf16x2(silu_fast(c0[0]), silu_fast(c0[1]));
-            a[kt][1] = pack_bf16x2(silu_fast(c0[2]), silu_fast(c0[3]));
-            a[kt][2] = pack_bf16x2(silu_fast(c1[0]), silu_fast(c1[1]));
-            a[kt][3] = pack_bf16x2(silu_fast(c1[2]), silu_fast(c1[3]));
+            a[kt][0] = silu_pack(c0[0], c0[1]);
+            a[kt][1] = silu_pack(c0[2], c0[3]);
+            a[kt][2] = silu_pack(c1[0], c1[1]);
+            a[kt][3] = silu_pack(c1[2], c1[3]);
         }
         // layer 2: [16 x 64] x [64 x 64] -> SiLU, two n-tiles at a time into
         // the A fragment of layer 3 ([16 x 64] x [64 x 8])
@@ -117,23 +140,19 @@ __device__ __forceinline__ void rows_forward(const Packed &P, float (*io)[4], in
                 mma_bf16_16816(c1, a[k2], P.w2[n1 + g][k2 * 8 + tg], P.w2[n1 + g][k2 * 8 + tg + 4]);
             }
             uint32_t a2[4];
-            a2[0] = pack_bf16x2(silu_fast(c0[0]), silu_fast(c0[1]));
-            a2[1] = pack_bf16x2(silu_fast(c0[2]), silu_fast(c0[3]));
-            a2[2] = pack_bf16x2(silu_fast(c1[0]), silu_fast(c1[1]));
-            a2[3] = pack_bf16x2(silu_fast(c1[2]), silu_fast(c1[3]));
+            a2[0] = silu_pack(c0[0], c0[1]);
+            a2[1] = silu_pack(c0[2], c0[3]);
+            a2[2] = silu_pack(c1[0], c1[1]);
+            a2[3] = silu_pack(c1[2], c1[3]);
             mma_bf16_16816(d, a2, P.w3[g][kt * 8 + tg], P.w3[g][kt * 8 + tg + 4]);
         }
-        out[mt][0] = d[0]; out[mt][1] = d[1]; out[mt][2] = d[2]; out[mt][3] = d[3];
-    }
-    __syncwarp();
-    // columns 2tg, 2tg+1 of rows g and g+8 of each m-tile; outputs 0..2 are in lanes with tg < 2
-    if (tg < 2) {
-#pragma unroll
-        for (int mt = 0; mt < 2; mt++) {
-            io[mt * 16 + g][2 * tg] = out[mt][0];
-            io[mt * 16 + g][2 * tg + 1] = out[mt][1];
-            io[mt * 16 + g + 8][2 * tg] = out[mt][2];
-            io[mt * 16 + g + 8][2 * tg + 1] = out[mt][3];
+        // this m-tile's rows were read into the A fragments before its first MMA:
+        // its outputs replace them (columns 2tg, 2tg+1 of rows g and g+8;
+        // outputs 0..2 are in the lanes with tg < 2)
+        __syncwarp();
+        if (tg < 2) {
+            io[r0][2 * tg] = d[0]; io[r0][2 * tg + 1] = d[1];
+            io[r1][2 * tg] = d[2]; io[r1][2 * tg + 1] = d[3];
         }
     }
     __syncwarp();

@@ -24,7 +24,8 @@
 //   k_mlp_forward   FP32 forward (evaluation, gradient checks)
 //   k_return_map_exact<Real>   the exact map on a batch of trial states
 //   k_return_map_learned       BF16 tensor-core inference (mma.sync
-//                   m16n8k16, FP32 accumulate, 32 samples per warp); trial
+//                   m16n8k16, FP32 accumulate, 32 samples per warp, the
+//                   fused kernel's network code, mlp_device.cuh); trial
 //                   states of cases 0-2 take the exact closed forms, case 3
 //                   takes the network, whose answer is kept only if it lies
 //                   on the yield surface within the tolerance, else the
@@ -225,59 +226,24 @@ __global__ void k_return_map_exact(MatT<T> m, const float4 *__restrict__ trial, 
     out[s] = make_float4(float(o1), float(o2), float(ojp), 0.0f);
 }
 
-__device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1)
-{
-    asm volatile("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-                 "{%0,%1,%2,%3};"
-                 : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-                 : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
-}
-
-__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi)
-{
-    const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
-    return *reinterpret_cast<const uint32_t *>(&v);
-}
-
-__device__ __forceinline__ float silu(float z) { return z * sigm(z); }
-
 constexpr int IWARPS = 8;
-
-struct InferSmem {
-    __nv_bfloat16 w1[HID][16];      // K padded 4 -> 16
-    __nv_bfloat16 w2[HID][HID];
-    __nv_bfloat16 w3[8][HID];       // N padded 3 -> 8
-    float b1[HID], b2[HID], b3[8];
-    float norm[14];
-    float x[IWARPS][32][IN];
-    float y[IWARPS][32][4];
-};
 
 // Learned map on a batch; out[s] = {sigma1', sigma2', Jp_inv', how} with how
 // 0 = exact closed form (cases 0-2), 1 = network accepted, 2 = exact after the
-// network's answer left the yield surface by more than `tol` (relative).
-__global__ void __launch_bounds__(IWARPS * 32) k_return_map_learned(MatT<float> m, const float *__restrict__ P,
+// network's answer left the yield surface by more than `tol` (relative).  The
+// network runs warp by warp on 32 trial states at a time (mlp::rows_forward,
+// the same code the fused kernel runs), the CTA's copy of it packed into
+// shared memory from the FP32 parameters at the start.
+__global__ void __launch_bounds__(IWARPS * 32, 2) k_return_map_learned(MatT<float> m, const float *__restrict__ P,
                                                                    const float *__restrict__ norm,
                                                                    const float4 *__restrict__ trial, int n,
                                                                    float tol, float4 *out, unsigned *fallbacks)
 {
-    __shared__ InferSmem sm;
+    __shared__ Smem<IWARPS> sm;
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-    for (int e = tid; e < HID * 16; e += blockDim.x) {
-        const int j = e / 16, i = e % 16;
-        sm.w1[j][i] = __float2bfloat16(i < IN ? P[W1 + j * IN + i] : 0.0f);
-    }
-    for (int e = tid; e < HID * HID; e += blockDim.x) sm.w2[e / HID][e % HID] = __float2bfloat16(P[W2 + e]);
-    for (int e = tid; e < 8 * HID; e += blockDim.x) {
-        const int o = e / HID, j = e % HID;
-        sm.w3[o][j] = __float2bfloat16(o < OUT ? P[W3 + o * HID + j] : 0.0f);
-    }
-    for (int e = tid; e < HID; e += blockDim.x) { sm.b1[e] = P[B1 + e]; sm.b2[e] = P[B2 + e]; }
-    if (tid < 8) sm.b3[tid] = tid < OUT ? P[B3 + tid] : 0.0f;
-    if (tid < 14) sm.norm[tid] = norm[tid];
+    for (int e = tid; e < PACK_ENTRIES; e += blockDim.x) pack_entry(e, P, norm, sm.p);
     __syncthreads();
-
-    const int g = lane >> 2, tg = lane & 3;
+    const float *nm = sm.p.norm;
     const long long nwarps = (long long)gridDim.x * IWARPS;
     for (long long base = ((long long)blockIdx.x * IWARPS + wid) * 32; base < n; base += nwarps * 32) {
         const long long s = base + lane;
@@ -289,84 +255,21 @@ __global__ void __launch_bounds__(IWARPS * 32) k_return_map_learned(MatT<float> 
         const float q = 2.0f * m.mu * fabsf(0.5f * (t.x * t.x - t.y * t.y)) / J;
         const int cs = return_map_case<float>(m, p, q, t.z);
         const bool use_net = valid && cs == 3 && t.x > 0.0f && t.y > 0.0f && t.z > 0.0f && t.w > 0.0f;
-        float xv[IN] = {logf(fmaxf(t.x, 1e-30f)), logf(fmaxf(t.y, 1e-30f)), logf(fmaxf(t.z, 1e-30f)),
-                        logf(fmaxf(t.w, 1e-30f))};
-#pragma unroll
-        for (int i = 0; i < IN; i++) sm.x[wid][lane][i] = (xv[i] - sm.norm[i]) / fmaxf(sm.norm[4 + i], 1e-30f);
-        __syncwarp();
-        if (__any_sync(0xffffffffu, use_net)) {
-            // layer 1: [32 x 16] x [16 x 64]
-            uint32_t a[2][4][4];     // A fragments of the next layer (k-tiles of 16)
-#pragma unroll
-            for (int mt = 0; mt < 2; mt++) {
-                uint32_t ax[4];
-                const int r0 = mt * 16 + g, r1 = r0 + 8;
-                ax[0] = tg < 2 ? pack_bf16(sm.x[wid][r0][2 * tg], sm.x[wid][r0][2 * tg + 1]) : 0u;
-                ax[1] = tg < 2 ? pack_bf16(sm.x[wid][r1][2 * tg], sm.x[wid][r1][2 * tg + 1]) : 0u;
-                ax[2] = 0u;
-                ax[3] = 0u;
-                float c[8][4];
-#pragma unroll
-                for (int nt = 0; nt < 8; nt++) {
-                    const int col = nt * 8 + 2 * tg;
-                    c[nt][0] = sm.b1[col]; c[nt][1] = sm.b1[col + 1];
-                    c[nt][2] = sm.b1[col]; c[nt][3] = sm.b1[col + 1];
-                    const uint32_t b0 = *reinterpret_cast<const uint32_t *>(&sm.w1[nt * 8 + g][2 * tg]);
-                    const uint32_t b1 = *reinterpret_cast<const uint32_t *>(&sm.w1[nt * 8 + g][2 * tg + 8]);
-                    mma_bf16(c[nt], ax, b0, b1);
-                }
-#pragma unroll
-                for (int kt = 0; kt < 4; kt++) {
-                    a[mt][kt][0] = pack_bf16(silu(c[2 * kt][0]), silu(c[2 * kt][1]));
-                    a[mt][kt][1] = pack_bf16(silu(c[2 * kt][2]), silu(c[2 * kt][3]));
-                    a[mt][kt][2] = pack_bf16(silu(c[2 * kt + 1][0]), silu(c[2 * kt + 1][1]));
-                    a[mt][kt][3] = pack_bf16(silu(c[2 * kt + 1][2]), silu(c[2 * kt + 1][3]));
-                }
-            }
-            // layer 2: [32 x 64] x [64 x 64], then layer 3: [32 x 64] x [64 x 8]
-#pragma unroll
-            for (int mt = 0; mt < 2; mt++) {
-                float c[8][4];
-#pragma unroll
-                for (int nt = 0; nt < 8; nt++) {
-                    const int col = nt * 8 + 2 * tg;
-                    c[nt][0] = sm.b2[col]; c[nt][1] = sm.b2[col + 1];
-                    c[nt][2] = sm.b2[col]; c[nt][3] = sm.b2[col + 1];
-#pragma unroll
-                    for (int kt = 0; kt < 4; kt++) {
-                        const uint32_t b0 = *reinterpret_cast<const uint32_t *>(&sm.w2[nt * 8 + g][kt * 16 + 2 * tg]);
-                        const uint32_t b1 =
-                            *reinterpret_cast<const uint32_t *>(&sm.w2[nt * 8 + g][kt * 16 + 2 * tg + 8]);
-                        mma_bf16(c[nt], a[mt][kt], b0, b1);
-                    }
-                }
-                float d[4] = {sm.b3[2 * tg], sm.b3[2 * tg + 1], sm.b3[2 * tg], sm.b3[2 * tg + 1]};
-#pragma unroll
-                for (int kt = 0; kt < 4; kt++) {
-                    uint32_t a2[4];
-                    a2[0] = pack_bf16(silu(c[2 * kt][0]), silu(c[2 * kt][1]));
-                    a2[1] = pack_bf16(silu(c[2 * kt][2]), silu(c[2 * kt][3]));
-                    a2[2] = pack_bf16(silu(c[2 * kt + 1][0]), silu(c[2 * kt + 1][1]));
-                    a2[3] = pack_bf16(silu(c[2 * kt + 1][2]), silu(c[2 * kt + 1][3]));
-                    const uint32_t b0 = *reinterpret_cast<const uint32_t *>(&sm.w3[g][kt * 16 + 2 * tg]);
-                    const uint32_t b1 = *reinterpret_cast<const uint32_t *>(&sm.w3[g][kt * 16 + 2 * tg + 8]);
-                    mma_bf16(d, a2, b0, b1);
-                }
-                if (tg < 2) {   // columns 0..3 of rows g and g+8 of this m-tile
-                    sm.y[wid][mt * 16 + g][2 * tg] = d[0];
-                    sm.y[wid][mt * 16 + g][2 * tg + 1] = d[1];
-                    sm.y[wid][mt * 16 + g + 8][2 * tg] = d[2];
-                    sm.y[wid][mt * 16 + g + 8][2 * tg + 1] = d[3];
-                }
-            }
+        float xin[IN] = {0.0f, 0.0f, 0.0f, 0.0f};
+        if (use_net) {
+            xin[0] = (logf(t.x) - nm[0]) / nm[4];
+            xin[1] = (logf(t.y) - nm[1]) / nm[5];
+            xin[2] = (logf(t.z) - nm[2]) / nm[6];
+            xin[3] = (logf(t.w) - nm[3]) / nm[7];
         }
-        __syncwarp();
+        float yo[OUT] = {0.0f, 0.0f, 0.0f};
+        if (__any_sync(0xffffffffu, use_net)) rows_forward(sm.p, sm.io[wid], lane, xin, yo);
         float o1 = t.x, o2 = t.y, ojp = t.z, how = 0.0f;
         bool fb = false;
         if (use_net) {
             float yv[OUT];
 #pragma unroll
-            for (int o = 0; o < OUT; o++) yv[o] = sm.y[wid][lane][o] * sm.norm[11 + o] + sm.norm[8 + o];
+            for (int o = 0; o < OUT; o++) yv[o] = yo[o] * nm[11 + o] + nm[8 + o];
             o1 = t.x * expf(yv[0]);
             o2 = t.y * expf(yv[1]);
             ojp = t.z * expf(yv[2]);
@@ -390,33 +293,18 @@ __global__ void __launch_bounds__(IWARPS * 32) k_return_map_learned(MatT<float> 
 }
 
 // FP32 master parameters and normalisation -> the packed network
-// (mlp_device.cuh), one thread per word.
+// (mlp_device.cuh), one thread per entry.
 __global__ void k_mlp_pack(const float *__restrict__ P, const float *__restrict__ norm, Packed *out)
 {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e < HID * 8) {                       // w1: k 2c, 2c+1 of row n (k >= IN is padding)
-        const int n = e / 8, c = e % 8, k = 2 * c;
-        out->w1[n][c] = pack_bf16x2(k < IN ? P[W1 + n * IN + k] : 0.0f, k + 1 < IN ? P[W1 + n * IN + k + 1] : 0.0f);
-    }
-    if (e < HID * HID / 2) {
-        const int n = e / (HID / 2), c = e % (HID / 2);
-        out->w2[n][c] = pack_bf16x2(P[W2 + n * HID + 2 * c], P[W2 + n * HID + 2 * c + 1]);
-    }
-    if (e < 8 * HID / 2) {                   // w3: rows n >= OUT are padding
-        const int n = e / (HID / 2), c = e % (HID / 2);
-        out->w3[n][c] = n < OUT ? pack_bf16x2(P[W3 + n * HID + 2 * c], P[W3 + n * HID + 2 * c + 1]) : 0u;
-    }
-    if (e < HID) { out->b1[e] = P[B1 + e]; out->b2[e] = P[B2 + e]; }
-    if (e < 8) out->b3[e] = e < OUT ? P[B3 + e] : 0.0f;
-    if (e < 16) out->norm[e] = e < 14 ? norm[e] : 0.0f;
+    if (e < PACK_ENTRIES) pack_entry(e, P, norm, *out);
 }
 
 }  // namespace mlp
 
 int mlp_pack(const float *d_params, const float *d_norm, void *d_packed, cudaStream_t stream)
 {
-    mlp::k_mlp_pack<<<(mlp::HID * mlp::HID / 2 + 255) / 256, 256, 0, stream>>>(d_params, d_norm,
-                                                                             (mlp::Packed *)d_packed);
+    mlp::k_mlp_pack<<<(mlp::PACK_ENTRIES + 255) / 256, 256, 0, stream>>>(d_params, d_norm, (mlp::Packed *)d_packed);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return fail(ICEMPM_E_CUDA, std::string("k_mlp_pack: ") + cudaGetErrorString(e));
     return ICEMPM_OK;

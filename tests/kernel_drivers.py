@@ -6,7 +6,8 @@ error bits).
     python tests/kernel_drivers.py frame [small]         # k_frame_scatter, k_frame_finish, k_blend_forcing
 
 ensemble: the first n_scenes (default 24) scenes of the ensemble generator in
-one batch, tile 512 nodes, one stage, direct launches, 5 + 3 sub-steps.
+one batch, the default kernel shape (no shared tile, two stages), direct
+launches, 5 + 3 sub-steps.
 frame: the floe-field scene (4096x2048, 23.0M points; `small`: the same rules
 on 2048x1024), 2 sub-steps, two current frames and a 64x128 wind grid, then
 three rounds of prepare_frame, set_forcing_time and get_forcing.
@@ -36,7 +37,7 @@ def ensemble(n_scenes):
     try:
         with capi.Batch(ctxs) as b:
             t = capi.BatchTuning()
-            t.tile_nodes, t.stages, t.sort_every, t.graph_steps = 512, 1, 0, 0
+            t.tile_nodes, t.stages, t.sort_every, t.graph_steps = 0, 2, 0, 0
             b.set_tuning(t)
             b.step(5, 0)
             b.step(3, 5)

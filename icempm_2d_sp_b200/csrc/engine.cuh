@@ -132,7 +132,7 @@ struct DevStatus {
     int32_t n_active;      // result slot of the compaction boundary search
     uint32_t err_pending;  // bits of the scatter for the next sub-step
     int32_t vc_step;       // G2P sub-step whose point velocity and C are stored
-    int32_t pad;
+    uint32_t chunk_ticket; // chunks of the fused kernel handed out beyond each CTA's first
 };
 
 template <class Real> struct Pts {
@@ -1000,6 +1000,7 @@ template <class Real, class Acc, int BT, int PPT, int CAP, int STAGES> struct Ch
     Stage stage[STAGES];
     Acc tile[3][CAP > 0 ? CAP : 1];
     unsigned long long mbar[2];
+    int nextc[2];           // chunk of the next iteration (the fused kernel's schedule)
     int red[BT / 32][5];
     int wbox[BT / 32][5];   // per warp: node box of its end patches {x0, x1, y0, y1}, duplicate cells
 };
@@ -1561,8 +1562,19 @@ k_g2p_p2g(KParams<Real> kp, Pts<Real> P, Grid<Real, Acc> G, DevStatus *st, int n
         mbar_fence_init();
     }
     __syncthreads();
+    // Chunk schedule: a CTA's first chunk is its block index; each later one
+    // is chunk gridDim.x + t for the next ticket t of st->chunk_ticket (rewound
+    // by the launch's last CTA), so that CTAs which finish their chunks early
+    // take more and the launch ends within about one chunk time on every SM.
+    // Thread 0 draws the ticket of iteration it + 2 while iteration it runs
+    // (the atomic's latency hides behind the chunk) and publishes the chunk of
+    // iteration it + 1 in sm.nextc[it & 1] before the iteration's barrier.
     int c = blockIdx.x;
-    if (tid == 0 && c < nchunks) fetch_chunk(sm.stage[0], P, (uint32_t)c * CH, CH, &sm.mbar[0], kp.tx_extra);
+    uint32_t ticket = 0;
+    if (tid == 0 && c < nchunks) {
+        fetch_chunk(sm.stage[0], P, (uint32_t)c * CH, CH, &sm.mbar[0], kp.tx_extra);
+        ticket = atomicAdd(&st->chunk_ticket, 1u);
+    }
 
     const int step = st->step;
     const bool recordPQ = kp.update_every > 0 && (step % kp.update_every) == 0;
@@ -1570,10 +1582,11 @@ k_g2p_p2g(KParams<Real> kp, Pts<Real> P, Grid<Real, Acc> G, DevStatus *st, int n
     uint32_t err = 0, perr = 0;
     int ndis = 0;
 
-    for (int it = 0; c < nchunks; it++, c += (int)gridDim.x) {
+    for (int it = 0; c < nchunks; it++) {
         const int s = STAGES == 2 ? (it & 1) : 0;
         const uint32_t parity = STAGES == 2 ? ((uint32_t)(it >> 1) & 1u) : ((uint32_t)it & 1u);
         const bool ok = mbar_wait_bounded(&sm.mbar[s], parity, kp.wait_ns);
+        if (tid == 0) sm.nextc[it & 1] = (int)min(gridDim.x + ticket, (uint32_t)nchunks);
         if (__syncthreads_or(!ok)) {
             // the chunk's copies did not complete in time: report it, give
             // copies still in flight one more bounded wait to land in this
@@ -1583,16 +1596,21 @@ k_g2p_p2g(KParams<Real> kp, Pts<Real> P, Grid<Real, Acc> G, DevStatus *st, int n
             __syncthreads();
             break;
         }
-        const bool next = c + (int)gridDim.x < nchunks;
-        const uint32_t base_n = (uint32_t)(c + (int)gridDim.x) * CH;
-        if (STAGES == 2 && tid == 0 && next)
-            fetch_chunk(sm.stage[s ^ 1], P, base_n, CH, &sm.mbar[s ^ 1], kp.tx_extra);
+        const int cn = sm.nextc[it & 1];
+        const bool next = cn < nchunks;
+        const uint32_t base_n = (uint32_t)cn * CH;
+        if (tid == 0 && next) {
+            if (STAGES == 2) fetch_chunk(sm.stage[s ^ 1], P, base_n, CH, &sm.mbar[s ^ 1], kp.tx_extra);
+            ticket = atomicAdd(&st->chunk_ticket, 1u);
+        }
         fused_chunk<Real, Acc, BT, PPT, CAP, STAGES, MODE>(sm, s, kp, P, G, (uint32_t)c * CH, n, step, recordPQ, store_vc,
                                                   next, P, base_n, err, perr, ndis, ml);
+        c = cn;
     }
     warp_flush_status(st, err, perr, ndis);
 
-    // the last CTA to finish advances the device step counter (no waiting)
+    // the last CTA to finish advances the device step counter and rewinds the
+    // chunk tickets for the next launch (no waiting)
     __syncthreads();
     if (tid == 0) {
         __threadfence();
@@ -1600,6 +1618,7 @@ k_g2p_p2g(KParams<Real> kp, Pts<Real> P, Grid<Real, Acc> G, DevStatus *st, int n
         if (t == gridDim.x - 1) {
             st->step = step + 1;
             st->done = 0;
+            st->chunk_ticket = 0;
             __threadfence();
         }
     }

@@ -12,11 +12,11 @@
 // (status >= 100 -> status - 99, else status).
 //
 // k_frame_scatter: four entries of the locality order per thread (one cell,
-// as the sort arranged them), their node terms summed in registers node by
-// node; each node's sums go straight to the global accumulators with three
-// 16-byte vector reductions (`red.global.add.v4.f32`): a node's eleven
-// channels (the ten above and the point count of its cell) are interleaved
-// in three float4.
+// as the sort arranged them), their node terms summed in registers column by
+// column and merged with the vertically adjacent lanes' overlapping nodes;
+// each node's sums go straight to the global accumulators with three 16-byte
+// vector reductions (`red.global.add.v4.f32`): a node's eleven channels (the
+// ten above and the point count of its cell) are interleaved in three float4.
 // k_frame_finish: one node per thread; region sums reduced in shared memory.
 #pragma once
 #include "engine.cuh"
@@ -71,13 +71,20 @@ __device__ __forceinline__ void frame_node_add(const FrameOut &F, int gy, int X,
 // A CTA takes 1024 entries of the locality order: 8 warps x 128, thread
 // (warp w, lane l) the entries w*128 + 32j + l, j = 0..3, which the sort put
 // in one cell.  When a thread's enabled points do share a cell, their node
-// terms are summed in registers first (three reductions per node for up to
-// four points); otherwise each point adds its own.
+// terms are summed in registers first, one column of three nodes at a time;
+// lanes whose cells are vertically adjacent in one column (lane l+1 one cell
+// above lane l, the usual case in the locality order) overlap in two of those
+// nodes, so each lane adds its upper neighbour's lowest node and its lower
+// neighbour's highest node into its centre node (warp shuffles) and writes a
+// corner node only where no neighbour took it: three reductions per node for
+// up to four points, and in a full column one node per column instead of
+// three.  A thread whose points span cells adds each point on its own.
 template <class Real>
-__global__ void __launch_bounds__(256) k_frame_scatter(Pts<Real> P, int n, int gx, int gy, Real particle_mass,
+__global__ void __launch_bounds__(256, 2) k_frame_scatter(Pts<Real> P, int n, int gx, int gy, Real particle_mass,
                                                        const uint32_t *__restrict__ colors, uint32_t ncolors,
                                                        FrameOut F)
 {
+    const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int e0 = blockIdx.x * 1024 + w * 128 + lane;
     bool act[4];
@@ -103,12 +110,24 @@ __global__ void __launch_bounds__(256) k_frame_scatter(Pts<Real> P, int n, int g
             else if (cxs[j] != cxs[first] || cys[j] != cys[first]) one_cell = false;
             nact++;
         }
-    if (nact > 0 && one_cell) {
+    const bool mine = nact > 0 && one_cell;
+    int cx = 0, cy = 0;
+#pragma unroll
+    for (int j = 0; j < 4; j++) if (j == first) { cx = cxs[j]; cy = cys[j]; }
+    const uint32_t key = mine ? (((uint32_t)cx << 16) | (uint32_t)cy) : 0xffffffffu;
+    const uint32_t key_up = __shfl_down_sync(FULL, key, 1);   // lane l+1
+    const uint32_t key_dn = __shfl_up_sync(FULL, key, 1);     // lane l-1
+    const bool above = mine && lane < 31 && key_up == key + 1u;
+    const bool below = mine && lane > 0 && key_dn == key - 1u;
+
+    // every lane takes part in the column loop (the shuffles); lanes without
+    // a one-cell patch carry zeros and write nothing
+    {
         float vals[4][kFrameChannels], wx[4][3], wy[4][3];
 #pragma unroll
         for (int j = 0; j < 4; j++) {
             float x = 0.0f, y = 0.0f;
-            if (act[j]) {
+            if (mine && act[j]) {
                 frame_values(P, e0 + 32 * j, particle_mass, colors, ncolors, vals[j], x, y);
                 bspline(x, wx[j]);
                 bspline(y, wy[j]);
@@ -119,23 +138,39 @@ __global__ void __launch_bounds__(256) k_frame_scatter(Pts<Real> P, int n, int g
                 for (int k = 0; k < 3; k++) { wx[j][k] = 0.0f; wy[j][k] = 0.0f; }
             }
         }
-        int cx = 0, cy = 0;
+#pragma unroll 1
+        for (int a = 0; a < 3; a++) {
+            float add[3][kFrameChannels + 1];   // nodes (a, 0..2): the ten channels and the point count
 #pragma unroll
-        for (int j = 0; j < 4; j++) if (j == first) { cx = cxs[j]; cy = cys[j]; }
-        for (int a = 0; a < 3; a++)
             for (int b = 0; b < 3; b++) {
-                float add[kFrameChannels];
 #pragma unroll
-                for (int c = 0; c < kFrameChannels; c++) add[c] = 0.0f;
-#pragma unroll
-                for (int j = 0; j < 4; j++) {
-                    const float wgt = wx[j][a] * wy[j][b];
-#pragma unroll
-                    for (int c = 0; c < kFrameChannels; c++) add[c] += wgt * vals[j][c];
-                }
-                frame_node_add(F, gy, cx + a - 1, cy + b - 1, add, (a == 1 && b == 1) ? float(nact) : 0.0f);
+                for (int c = 0; c < kFrameChannels; c++) add[b][c] = 0.0f;
+                add[b][kFrameChannels] = (a == 1 && b == 1) ? float(nact) : 0.0f;
             }
-    } else if (nact > 0) {
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const float wa = a == 0 ? wx[j][0] : (a == 1 ? wx[j][1] : wx[j][2]);   // registers, not a stack array
+#pragma unroll
+                for (int b = 0; b < 3; b++) {
+                    const float wgt = wa * wy[j][b];
+#pragma unroll
+                    for (int c = 0; c < kFrameChannels; c++) add[b][c] += wgt * vals[j][c];
+                }
+            }
+#pragma unroll
+            for (int c = 0; c <= kFrameChannels; c++) {
+                const float up = __shfl_down_sync(FULL, add[0][c], 1), dn = __shfl_up_sync(FULL, add[2][c], 1);
+                if (above) add[1][c] += up;
+                if (below) add[1][c] += dn;
+            }
+            if (mine) {
+                frame_node_add(F, gy, cx + a - 1, cy, add[1], add[1][kFrameChannels]);
+                if (!below) frame_node_add(F, gy, cx + a - 1, cy - 1, add[0], add[0][kFrameChannels]);
+                if (!above) frame_node_add(F, gy, cx + a - 1, cy + 1, add[2], add[2][kFrameChannels]);
+            }
+        }
+    }
+    if (nact > 0 && !one_cell) {
 #pragma unroll 1
         for (int j = 0; j < 4; j++) {
             if (!act[j]) continue;

@@ -249,7 +249,7 @@ static __global__ void k_set_step(DevStatus *st, int step, int reset_done, int n
 {
     if (step >= 0) st->step = step;
     st->vc_step = st->step + nsteps - 1;
-    if (reset_done) st->done = 0;
+    if (reset_done) { st->done = 0; st->chunk_ticket = 0; }
 }
 
 }  // namespace icempm

@@ -337,6 +337,17 @@ def combine_ranks(dist, t_ms, n):
     return float(t.item()), int(c.item())
 
 
+def sum_ranks(dist, x):
+    """Sum of a per-rank figure over the ranks (x itself for one process)."""
+    if dist is None:
+        return x
+    import torch
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(x)], device=dev, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -435,6 +446,11 @@ def main():
     e2e = None
     if not args.no_e2e:
         e2e = end_to_end(args, sc, local, capi, Options, VARIANT_FIXED)
+        # whole job: the slowest rank's wall time, all ranks' points and copies
+        t_e2e, n_e2e = combine_ranks(dist, e2e.pop("seconds") * 1e3, n)
+        e2e["value"] = n_e2e * args.steps / (t_e2e * 1e-3)
+        e2e["h2d_bytes_per_step"] = sum_ranks(dist, e2e["h2d_bytes_per_step"])
+        e2e["d2h_bytes_per_step"] = sum_ranks(dist, e2e["d2h_bytes_per_step"])
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -534,7 +550,7 @@ def end_to_end(args, sc, local, capi, Options, variant):
         for b in [src, fbuf] + dst:
             capi.host_unregister(b)
     hssoa_bytes = 19 * 8 * n
-    return {"value": n * args.steps / (t1 - t0), "unit": UNIT,
+    return {"value": n * args.steps / (t1 - t0), "unit": UNIT, "seconds": t1 - t0,
             "h2d_bytes_per_step": hssoa_bytes / args.steps,
             "d2h_bytes_per_step": frames * (hssoa_bytes + 16 * G + 8) / args.steps,
             "frames": frames, "frame_steps": frame,

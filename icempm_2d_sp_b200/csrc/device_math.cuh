@@ -77,11 +77,9 @@ __device__ __forceinline__ double2 pfma(double2 a, double2 b, double2 c)
 
 // B-spline weights of both components of a pair: w[k] = (w_k(v.x), w_k(v.y)).
 // With v = (x, x) every w[k] is a broadcast pair.  w[1] = 0.75 - x^2 is
-// formed as (0.5 - x)(x + 0.5) + 0.5.
-template <class PT> __device__ __forceinline__ void bspline2(PT v, PT w[3])
+// formed as (0.5 - x)(x + 0.5) + 0.5.  `half` is the pair (0.5, 0.5).
+template <class PT> __device__ __forceinline__ void bspline2(PT v, PT w[3], PT half)
 {
-    using T = decltype(v.x);
-    const PT half = pbc(T(0.5));
     const PT v0 = psub(half, v), v2 = padd(v, half);
     w[0] = pmul(pmul(half, v0), v0);
     w[1] = pfma(v0, v2, half);

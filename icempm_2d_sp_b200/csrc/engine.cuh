@@ -197,6 +197,13 @@ template <class Real> struct KParams {
     const mlp::Packed *mlp;         // learned return map (the LEARNED instance): packed network
     float mlp_tol;                  // ... accepted when its answer lies on the yield surface within this
     unsigned long long *mlp_counts; // ... [0] answers kept, [1] exact fallbacks
+    // Broadcast pairs of the factors the packed arithmetic of the fused
+    // kernel uses (one 8-byte constant load each, no register shuffling):
+    // dt/h, -4/h, -h, 1, 1/2, the extended forcing's impulse factor, and the
+    // fixed-point scales (1 for float accumulators): momentum scale, h times
+    // it, mass scale (scalar).
+    P2<Real> dt_h_inv2, neg_four_h_inv2, neg_h2, one2, half2, ext_impulse2, sp2, hsp2;
+    Real sm_r;
 };
 
 // Fire-and-forget reductions into global memory (red.global: no value comes
@@ -929,12 +936,13 @@ template <class Real> struct SrcP {
 };
 
 // The node terms, summed separably over the weights of both axes.
-template <class Real> __device__ __forceinline__ void patch_accumulate(Patch<Real> &p, const SrcP<Real> &s)
+template <class Real>
+__device__ __forceinline__ void patch_accumulate(Patch<Real> &p, const SrcP<Real> &s, P2<Real> half)
 {
     using PT = P2<Real>;
     PT wx[3], wy[3];
-    bspline2(pbc(s.x), wx);
-    bspline2(pbc(s.y), wy);
+    bspline2(pbc(s.x), wx, half);
+    bspline2(pbc(s.y), wy, half);
     const PT axa[3] = {psub(s.A, s.S0), s.A, padd(s.A, s.S0)};
 #pragma unroll
     for (int a = 0; a < 3; a++) {
@@ -952,7 +960,7 @@ template <class Real> __device__ __forceinline__ void patch_accumulate(Patch<Rea
 
 template <class Real, class Acc, int CAP>
 __device__ __forceinline__ void patch_add(Patch<Real> &p, const SrcP<Real> &s, const Tile<Acc, CAP> &T,
-                                          const AccGrid<Acc> &gacc, int gy)
+                                          const AccGrid<Acc> &gacc, int gy, P2<Real> half)
 {
     if (p.have) {
         const bool same = s.cx == p.cx && s.cy == p.cy;
@@ -979,7 +987,7 @@ __device__ __forceinline__ void patch_add(Patch<Real> &p, const SrcP<Real> &s, c
         p.in_tile = cell_in_tile(T, s.cx, s.cy);
         p.have = true;
     }
-    patch_accumulate(p, s);
+    patch_accumulate(p, s, half);
 }
 
 // Shared memory of one CTA of the fused kernel.  A chunk is CH = BT*PPT
@@ -1144,7 +1152,10 @@ __device__ __noinline__ void learned_projection(const KParams<Real> &kp, mlp::Sm
 // that records return-map pairs, FUSED_LEARNED the one whose projections onto
 // the yield surface go to the learned return map (both kept out of the
 // ordinary instance, whose registers they would crowd); ml is the learned
-// map's shared memory (FUSED_LEARNED only).
+// map's shared memory (FUSED_LEARNED only).  SCENES: kp lives in shared
+// memory (the scene-table kernel), where the pairs (1, 1) and (1/2, 1/2) are
+// formed from immediates instead (the register allocation of that kernel
+// spills more with them loaded from kp).
 //
 // G2P follows partition_kernel_g2p (kernels.cuh:181-315), P2G
 // partition_kernel_p2g (kernels.cuh:39-104).  Two phases per chunk:
@@ -1169,7 +1180,7 @@ __device__ __noinline__ void learned_projection(const KParams<Real> &kp, mlp::Sm
 // cancels because sum_a wx_a (a-1-x) = 0 and sum_b wy_b (b-1-y) = 0) and keeps
 // FP32 roundoff relative to velocity differences.  Velocities, momenta and
 // the columns of C are pairs (packed FP32x2 arithmetic).
-template <class Real, class Acc, int BT, int PPT, int CAP, int STAGES, int MODE>
+template <class Real, class Acc, int BT, int PPT, int CAP, int STAGES, int MODE, bool SCENES = false>
 __device__ __forceinline__ void fused_chunk(ChunkSmem<Real, Acc, BT, PPT, CAP, STAGES> &sm, int s,
                                             const KParams<Real> &kp, const Pts<Real> &P, const Grid<Real, Acc> &G,
                                             uint32_t base, int n, int step, bool recordPQ, bool store_vc, bool next,
@@ -1185,6 +1196,7 @@ __device__ __forceinline__ void fused_chunk(ChunkSmem<Real, Acc, BT, PPT, CAP, S
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     typename SM::Stage &sg = sm.stage[s];
     const int wbase = wid * 32 * PPT + lane;
+    const PT one = SCENES ? pbc(Real(1)) : kp.one2, half = SCENES ? pbc(Real(0.5)) : kp.half2;
 
     // ---- phase 1 ----------------------------------------------------------
     unsigned xmn = 0xffffu, ymn = 0xffffu, xmx = 0, ymx = 0;   // box of the new cells that scatter
@@ -1243,13 +1255,15 @@ __device__ __forceinline__ void fused_chunk(ChunkSmem<Real, Acc, BT, PPT, CAP, S
                 }
                 // column sums first (weights of y), then the row combination (weights of x),
                 // so that only one axis's weight pairs are live at a time
-                const PT one = pbc(Real(1));
+                // (the gradient weights are taken with the opposite sign,
+                // wy_b (y - (b-1)), which makes ta, pv and qv the negatives of
+                // the sums above, exactly; -4/h restores the sign of C)
                 PT sa[3], ta[3];
                 {
                     PT wy[3];
-                    bspline2(pbc(A.y), wy);
-                    const PT ny = pbc(-A.y);
-                    const PT gy[3] = {pmul(wy[0], psub(ny, one)), pmul(wy[1], ny), pmul(wy[2], padd(ny, one))};
+                    const PT vy = pbc(A.y);
+                    bspline2(vy, wy, half);
+                    const PT gy[3] = {pmul(wy[0], padd(vy, one)), pmul(wy[1], vy), pmul(wy[2], psub(vy, one))};
                     // a = 0: dv[0..2] are nodes (0, 0..2); a = 1: dv[3], dv[4] are nodes (1, 0), (1, 2)
                     // (the centre's difference is zero); a = 2: dv[5..7] are nodes (2, 0..2)
                     sa[0] = pfma(wy[2], dv[2], pfma(wy[1], dv[1], pmul(wy[0], dv[0])));
@@ -1262,19 +1276,18 @@ __device__ __forceinline__ void fused_chunk(ChunkSmem<Real, Acc, BT, PPT, CAP, S
                 PT sv, pv, qv;
                 {
                     PT wx[3];
-                    bspline2(pbc(A.x), wx);
-                    const PT nx = pbc(-A.x);
-                    const PT gx[3] = {pmul(wx[0], psub(nx, one)), pmul(wx[1], nx), pmul(wx[2], padd(nx, one))};
+                    const PT vx = pbc(A.x);
+                    bspline2(vx, wx, half);
+                    const PT gx[3] = {pmul(wx[0], padd(vx, one)), pmul(wx[1], vx), pmul(wx[2], psub(vx, one))};
                     sv = pfma(wx[2], sa[2], pfma(wx[1], sa[1], pmul(wx[0], sa[0])));
                     pv = pfma(gx[2], sa[2], pfma(gx[1], sa[1], pmul(gx[0], sa[0])));
                     qv = pfma(wx[2], ta[2], pfma(wx[1], ta[1], pmul(wx[0], ta[0])));
                 }
                 v = padd(vc, sv);
-                const PT fh = pbc(kp.four_h_inv);
-                c0 = pmul(fh, pv);
-                c1 = pmul(fh, qv);
+                c0 = pmul(kp.neg_four_h_inv2, pv);
+                c1 = pmul(kp.neg_four_h_inv2, qv);
             }
-            const PT xy = pfma(v, pbc(kp.dt_h_inv), pmk(A.x, A.y));
+            const PT xy = pfma(v, kp.dt_h_inv2, pmk(A.x, A.y));
             {   // one test in the usual case; a NaN in any of the sums reaches the total
                 const PT t = padd(padd(v, xy), padd(c0, c1));
                 if (isnan(t.x + t.y)) {
@@ -1284,15 +1297,17 @@ __device__ __forceinline__ void fused_chunk(ChunkSmem<Real, Acc, BT, PPT, CAP, S
                 }
             }
             x = xy.x; y = xy.y;
-            if (x > Real(0.5)) { x -= Real(1); cx++; moved = true; }
-            else if (x < Real(-0.5)) { x += Real(1); cx--; moved = true; }
-            if (y > Real(0.5)) { y -= Real(1); cy++; moved = true; }
-            else if (y < Real(-0.5)) { y += Real(1); cy--; moved = true; }
-            if (moved && (cx <= 1 || cx >= kp.gx - 2 || cy <= 1 || cy >= kp.gy - 2)) {
-                util |= kDisabled;
-                ndis++;
+            if (fabs(x) > Real(0.5) || fabs(y) > Real(0.5)) {   // the point left its cell (rare)
+                if (x > Real(0.5)) { x -= Real(1); cx++; moved = true; }
+                else if (x < Real(-0.5)) { x += Real(1); cx--; moved = true; }
+                if (y > Real(0.5)) { y -= Real(1); cy++; moved = true; }
+                else if (y < Real(-0.5)) { y += Real(1); cy--; moved = true; }
+                if (moved && (cx <= 1 || cx >= kp.gx - 2 || cy <= 1 || cy >= kp.gy - 2)) {
+                    util |= kDisabled;
+                    ndis++;
+                }
+                if (x > Real(0.5) || x < Real(-0.5) || y > Real(0.5) || y < Real(-0.5)) err |= kErrJump;
             }
-            if (x > Real(0.5) || x < Real(-0.5) || y > Real(0.5) || y < Real(-0.5)) err |= kErrJump;
 
             // Fe <- (I + dt C) Fe, i.e. H <- H + D + D H with D = dt C
             {
@@ -1361,18 +1376,15 @@ __device__ __forceinline__ void fused_chunk(ChunkSmem<Real, Acc, BT, PPT, CAP, S
                     const PT nsc = pbc(-(kp.dt_vol_Dpinv * Jp * thick)), mpp = pbc(mp);
                     const PT S0 = pfma(mpp, c0, pmul(nsc, pmk(tau.a00, tau.a10)));
                     const PT S1 = pfma(mpp, c1, pmul(nsc, pmk(tau.a01, tau.a11)));
-                    PT Av = pfma(pbc(-kp.h), pfma(S0, pbc(x), pmul(S1, pbc(y))), pmul(mpp, v));
+                    PT Av = pfma(kp.neg_h2, pfma(S0, pbc(x), pmul(S1, pbc(y))), pmul(mpp, v));
                     if (kp.ext) {   // wind stress and current of the new cell's node
                         const V4<Real> f = moved ? G.frc[(uint32_t)cx * (uint32_t)kp.gy + (uint32_t)cy] : fc;
                         const PT d = psub(pmk(f.x, f.y), v);
                         const Real cw = kp.rho_w_cd * tsqrt(d.x * d.x + d.y * d.y);
-                        Av = pfma(pbc(kp.ext_impulse), pfma(pbc(cw), d, pmk(f.z, f.w)), Av);
+                        Av = pfma(kp.ext_impulse2, pfma(pbc(cw), d, pmk(f.z, f.w)), Av);
                     }
-                    const Real fm = FIXED ? Real(kp.scale_m) : Real(1);
-                    const Real fp = FIXED ? Real(kp.scale_p) : Real(1);
-                    const PT hp = pbc(kp.h * fp);
-                    const PT sA = pmul(Av, pbc(fp)), sS0 = pmul(hp, S0), sS1 = pmul(hp, S1);
-                    const Real smp = mp * fm;
+                    const PT sA = pmul(Av, kp.sp2), sS0 = pmul(kp.hsp2, S0), sS1 = pmul(kp.hsp2, S1);
+                    const Real smp = mp * kp.sm_r;
                     // Fixed point: a node term is at most max(w) <= 0.5625 times the
                     // bounds below.  Finite sources with |x|, |y| <= 2 raise no P2G
                     // bit; anything else takes the exact tests.
@@ -1455,7 +1467,7 @@ __device__ __forceinline__ void fused_chunk(ChunkSmem<Real, Acc, BT, PPT, CAP, S
         src.x = a4.x; src.y = a4.y;
         src.mp = get_src_mass<Real>(sg, local, k2);
         src.A = pmk(h4.x, h4.y); src.S0 = pmk(h4.z, h4.w); src.S1 = pmk(a4.z, a4.w);
-        patch_add<Real, Acc, CAP>(patch, src, T, G.acc, kp.gy);
+        patch_add<Real, Acc, CAP>(patch, src, T, G.acc, kp.gy, half);
     }
     // end patches: merge neighbours, then write them out.  Without a tile
     // (CAP == 0) every node goes straight to the global accumulators (one
@@ -1712,7 +1724,7 @@ k_g2p_p2g_batch(const SceneDesc<Real, Acc> *__restrict__ scenes, const int *__re
         const uint32_t base_n = (uint32_t)(cn - Sn.chunk0) * CH;
         if (STAGES == 2 && tid == 0 && next) fetch_chunk(sm.stage[s ^ 1], Sn.P, base_n, CH, &sm.mbar[s ^ 1]);
         const bool recordPQ = S.kp.update_every > 0 && (step % S.kp.update_every) == 0;
-        fused_chunk<Real, Acc, BT, PPT, CAP, STAGES, FUSED_PLAIN>(sm, s, S.kp, S.P, S.G, (uint32_t)(c - S.chunk0) * CH, S.n,
+        fused_chunk<Real, Acc, BT, PPT, CAP, STAGES, FUSED_PLAIN, true>(sm, s, S.kp, S.P, S.G, (uint32_t)(c - S.chunk0) * CH, S.n,
                                                           step, recordPQ, store_vc, next, Sn.P, base_n, err, perr, ndis);
         warp_flush_status(S.st, err, perr, ndis);
     }

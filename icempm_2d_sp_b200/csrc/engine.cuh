@@ -274,7 +274,8 @@ __device__ __forceinline__ void warp_flush_status(DevStatus *st, uint32_t err, u
 
 __device__ __forceinline__ bool cell_in_range(int cx, int cy, int gx, int gy)
 {
-    return cx >= 1 && cx <= gx - 2 && cy >= 1 && cy <= gy - 2;
+    // 1 <= cx <= gx - 2 and 1 <= cy <= gy - 2, as two unsigned compares (grids are >= 5 nodes a side)
+    return (uint32_t)(cx - 1) <= (uint32_t)(gx - 3) && (uint32_t)(cy - 1) <= (uint32_t)(gy - 3);
 }
 
 // ---- P2G sources of one point --------------------------------------------
@@ -840,6 +841,7 @@ template <class Real> struct Patch {
     Real m[3][3];
     P2<Real> p[3][3];
     int cx, cy;
+    uint32_t key;   // (cy << 16) | cx while `have`; kNoScatter before
     bool have, in_tile;
 };
 
@@ -958,9 +960,11 @@ __device__ __forceinline__ void patch_accumulate(Patch<Real> &p, const SrcP<Real
     }
 }
 
+// Moves the patch to the source's cell (s.cx, s.cy), which differs from its
+// own: a slide by one cell up, or a flush and a fresh patch.
 template <class Real, class Acc, int CAP>
-__device__ __forceinline__ void patch_add(Patch<Real> &p, const SrcP<Real> &s, const Tile<Acc, CAP> &T,
-                                          const AccGrid<Acc> &gacc, int gy, P2<Real> half)
+__device__ __forceinline__ void patch_move(Patch<Real> &p, const SrcP<Real> &s, const Tile<Acc, CAP> &T,
+                                           const AccGrid<Acc> &gacc, int gy)
 {
     if (p.have) {
         const bool same = s.cx == p.cx && s.cy == p.cy;
@@ -987,7 +991,7 @@ __device__ __forceinline__ void patch_add(Patch<Real> &p, const SrcP<Real> &s, c
         p.in_tile = cell_in_tile(T, s.cx, s.cy);
         p.have = true;
     }
-    patch_accumulate(p, s, half);
+    p.key = ((uint32_t)p.cy << 16) | (uint32_t)p.cx;
 }
 
 // Shared memory of one CTA of the fused kernel.  A chunk is CH = BT*PPT
@@ -1212,17 +1216,16 @@ __device__ __forceinline__ void fused_chunk(ChunkSmem<Real, Acc, BT, PPT, CAP, S
         const uint2 key = inb ? sg.K[local] : make_uint2(0u, kDisabled);
         uint32_t util = key.y;
         const bool act = !(util & kDisabled);
-        if (inb && !act) sg.K[local].x = kNoScatter;
-        if (MODE != FUSED_LEARNED && !act) {
-            if (!inb) break;
-            continue;
-        }
+        // entries that scatter nothing (disabled points, and in the last chunk
+        // the entries past n) are marked so in the stage, for phase 2
+        if (!act) sg.K[local].x = kNoScatter;
+        if (MODE != FUSED_LEARNED && !act) continue;
         // The learned instance keeps every lane in the loop body (inactive
         // lanes with act = false), so that the warp meets at the network.
         Real x = Real(0), y = Real(0), Jp = Real(0), thick = Real(0);
         M2<Real> H = {Real(0), Real(0), Real(0), Real(0)};
         int cx = 0, cy = 0;
-        bool moved = false;
+        bool moved = false, in0 = false;   // in0: the start cell is in range
         PT v = pbc(Real(0)), c0 = pbc(Real(0)), c1 = pbc(Real(0));   // (vx, vy), (c00, c10), (c01, c11)
         Kin<Real> k{};
         Real p_tr = Real(0), q_tr = Real(0);
@@ -1235,7 +1238,8 @@ __device__ __forceinline__ void fused_chunk(ChunkSmem<Real, Acc, BT, PPT, CAP, S
             thick = A.w;
             H = {Hv.x, Hv.y, Hv.z, Hv.w};
             cx = (int)(key.x & 0xffff); cy = (int)(key.x >> 16);
-            if (cell_in_range(cx, cy, kp.gx, kp.gy)) {
+            in0 = cell_in_range(cx, cy, kp.gx, kp.gy);
+            if (in0) {
                 if (!ICEMPM_VEL_CACHE || key.x != vcell) {
                     vcell = key.x;
                     const V2<Real> *col = G.vel + ((uint32_t)(cx - 1) * (uint32_t)kp.gy + (uint32_t)(cy - 1));
@@ -1370,7 +1374,7 @@ __device__ __forceinline__ void fused_chunk(ChunkSmem<Real, Acc, BT, PPT, CAP, S
             // A = m_p v - h (S0 x + S1 y) (+ the extended forcing's impulse).
             uint2 src_key = make_uint2(kNoScatter, 0u);   // new cell and mass of the source, or no scatter
             if (!(util & kDisabled)) {
-                if (cell_in_range(cx, cy, kp.gx, kp.gy)) {
+                if (moved ? cell_in_range(cx, cy, kp.gx, kp.gy) : in0) {
                     const M2<Real> tau = kirchhoff(k, kp.mat.mu, kp.mat.kappa);
                     const Real mp = kp.particle_mass * thick;
                     const PT nsc = pbc(-(kp.dt_vol_Dpinv * Jp * thick)), mpp = pbc(mp);
@@ -1453,21 +1457,23 @@ __device__ __forceinline__ void fused_chunk(ChunkSmem<Real, Acc, BT, PPT, CAP, S
 
     // ---- phase 2 ----------------------------------------------------------
     Patch<Real> patch;
-    patch.have = false; patch.in_tile = false; patch.cx = patch.cy = 0;
+    patch.have = false; patch.in_tile = false; patch.cx = patch.cy = 0; patch.key = kNoScatter;
 #pragma unroll
     for (int j = 0; j < PPT; j++) {
         const int local = wbase + 32 * j;
-        if (base + (uint32_t)local >= (uint32_t)n) break;
         const uint2 k2 = sg.K[local];
         if (k2.x == kNoScatter) continue;
         const V4<Real> a4 = sg.A[local];
         const V4<Real> h4 = sg.H[local];
         SrcP<Real> src;
-        src.cx = (int)(k2.x & 0xffff); src.cy = (int)(k2.x >> 16);
         src.x = a4.x; src.y = a4.y;
         src.mp = get_src_mass<Real>(sg, local, k2);
         src.A = pmk(h4.x, h4.y); src.S0 = pmk(h4.z, h4.w); src.S1 = pmk(a4.z, a4.w);
-        patch_add<Real, Acc, CAP>(patch, src, T, G.acc, kp.gy, half);
+        if (k2.x != patch.key) {   // the first source, or one from another cell (rare)
+            src.cx = (int)(k2.x & 0xffff); src.cy = (int)(k2.x >> 16);
+            patch_move<Real, Acc, CAP>(patch, src, T, G.acc, kp.gy);
+        }
+        patch_accumulate(patch, src, half);
     }
     // end patches: merge neighbours, then write them out.  Without a tile
     // (CAP == 0) every node goes straight to the global accumulators (one

@@ -1587,10 +1587,14 @@ k_g2p_p2g(KParams<Real> kp, Pts<Real> P, Grid<Real, Acc> G, DevStatus *st, int n
     // Thread 0 draws the ticket of iteration it + 2 while iteration it runs
     // (the atomic's latency hides behind the chunk) and publishes the chunk of
     // iteration it + 1 in sm.nextc[it & 1] before the iteration's barrier.
+    // Schedule position c processes the chunk nchunks - 1 - c: the points
+    // (sorted by cell) are walked from the high cells down, starting where
+    // the grid update, which walks the nodes upwards, has just left its
+    // velocities and cleared accumulators in L2.
     int c = blockIdx.x;
     uint32_t ticket = 0;
     if (tid == 0 && c < nchunks) {
-        fetch_chunk(sm.stage[0], P, (uint32_t)c * CH, CH, &sm.mbar[0], kp.tx_extra);
+        fetch_chunk(sm.stage[0], P, (uint32_t)(nchunks - 1 - c) * CH, CH, &sm.mbar[0], kp.tx_extra);
         ticket = atomicAdd(&st->chunk_ticket, 1u);
     }
 
@@ -1616,12 +1620,13 @@ k_g2p_p2g(KParams<Real> kp, Pts<Real> P, Grid<Real, Acc> G, DevStatus *st, int n
         }
         const int cn = sm.nextc[it & 1];
         const bool next = cn < nchunks;
-        const uint32_t base_n = (uint32_t)cn * CH;
+        const uint32_t base_n = (uint32_t)(nchunks - 1 - cn) * CH;   // used only with next
         if (tid == 0 && next) {
             if (STAGES == 2) fetch_chunk(sm.stage[s ^ 1], P, base_n, CH, &sm.mbar[s ^ 1], kp.tx_extra);
             ticket = atomicAdd(&st->chunk_ticket, 1u);
         }
-        fused_chunk<Real, Acc, BT, PPT, CAP, STAGES, MODE>(sm, s, kp, P, G, (uint32_t)c * CH, n, step, recordPQ, store_vc,
+        fused_chunk<Real, Acc, BT, PPT, CAP, STAGES, MODE>(sm, s, kp, P, G, (uint32_t)(nchunks - 1 - c) * CH, n, step,
+                                                  recordPQ, store_vc,
                                                   next, P, base_n, err, perr, ndis, ml);
         c = cn;
     }
@@ -1693,16 +1698,20 @@ k_g2p_p2g_batch(const SceneDesc<Real, Acc> *__restrict__ scenes, const int *__re
         mbar_fence_init();
     }
     __syncthreads();
+    // schedule position c processes the chunk nchunks - 1 - c (high cells of
+    // the last scene first: see k_g2p_p2g)
     int c = blockIdx.x;
     if (tid == 0 && c < nchunks) {
-        const SceneDesc<Real, Acc> &S0 = scenes[chunk_scene[c]];
-        fetch_chunk(sm.stage[0], S0.P, (uint32_t)(c - S0.chunk0) * CH, CH, &sm.mbar[0]);
+        const int cc = nchunks - 1 - c;
+        const SceneDesc<Real, Acc> &S0 = scenes[chunk_scene[cc]];
+        fetch_chunk(sm.stage[0], S0.P, (uint32_t)(cc - S0.chunk0) * CH, CH, &sm.mbar[0]);
     }
     const int step = bst->step;
     const bool store_vc = step == bst->vc_step;
 
     for (int it = 0; c < nchunks; it++, c += (int)gridDim.x) {
-        const int sc = chunk_scene[c];
+        const int cc = nchunks - 1 - c;
+        const int sc = chunk_scene[cc];
         if (sc != cur_scene) {   // block-uniform: every thread of the CTA walks the same chunks
             __syncthreads();
             static_assert(sizeof(SceneDesc<Real, Acc>) % 4 == 0, "word copy");
@@ -1726,11 +1735,12 @@ k_g2p_p2g_batch(const SceneDesc<Real, Acc> *__restrict__ scenes, const int *__re
         }
         const int cn = c + (int)gridDim.x;
         const bool next = cn < nchunks;
-        const SceneDesc<Real, Acc> &Sn = scenes[chunk_scene[next ? cn : c]];
-        const uint32_t base_n = (uint32_t)(cn - Sn.chunk0) * CH;
+        const int ccn = next ? nchunks - 1 - cn : cc;
+        const SceneDesc<Real, Acc> &Sn = scenes[chunk_scene[ccn]];
+        const uint32_t base_n = (uint32_t)(ccn - Sn.chunk0) * CH;
         if (STAGES == 2 && tid == 0 && next) fetch_chunk(sm.stage[s ^ 1], Sn.P, base_n, CH, &sm.mbar[s ^ 1]);
         const bool recordPQ = S.kp.update_every > 0 && (step % S.kp.update_every) == 0;
-        fused_chunk<Real, Acc, BT, PPT, CAP, STAGES, FUSED_PLAIN, true>(sm, s, S.kp, S.P, S.G, (uint32_t)(c - S.chunk0) * CH, S.n,
+        fused_chunk<Real, Acc, BT, PPT, CAP, STAGES, FUSED_PLAIN, true>(sm, s, S.kp, S.P, S.G, (uint32_t)(cc - S.chunk0) * CH, S.n,
                                                           step, recordPQ, store_vc, next, Sn.P, base_n, err, perr, ndis);
         warp_flush_status(S.st, err, perr, ndis);
     }

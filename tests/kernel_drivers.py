@@ -4,6 +4,7 @@ error bits).
 
     python tests/kernel_drivers.py ensemble [n_scenes]   # k_g2p_p2g_batch, k_grid_update_batch
     python tests/kernel_drivers.py frame [small]         # k_frame_scatter, k_frame_finish, k_blend_forcing
+    python tests/kernel_drivers.py learned               # k_return_map_learned, k_return_map_exact
 
 ensemble: the first n_scenes (default 24) scenes of the ensemble generator in
 one batch, the default kernel shape (no shared tile, two stages), direct
@@ -11,6 +12,10 @@ launches, 5 + 3 sub-steps.
 frame: the floe-field scene (4096x2048, 23.0M points; `small`: the same rules
 on 2048x1024), 2 sub-steps, two current frames and a 64x128 wind grid, then
 three rounds of prepare_frame, set_forcing_time and get_forcing.
+learned: projections harvested from 40 sub-steps of a 256x128 ridging scene,
+a network trained on them for 4 epochs, then the batch maps on 10M trial
+states (the harvested ones repeated; every row a projection): the exact map
+and the learned map at tolerance 1e-2, three calls each.
 """
 import os
 import sys
@@ -75,13 +80,32 @@ def frame(small):
     return 1 if err else 0
 
 
+def learned():
+    from icempm_2d_sp_b200 import surrogate
+    sc = scenes.ridging(gx=256, gy=128, cells_x=120, cells_y=100, speed=2.0)
+    with capi.Context(sc.prms, sc.status, sc.current, capacity=sc.n, options=Options.default()) as ctx:
+        ctx.upload(sc.soa, sc.n)
+        ctx.harvest_begin(400_000, stride=1)
+        ctx.step(40, 0)
+        rec, _ = ctx.harvest_end()
+    params, norm, _ = surrogate.train(rec, epochs=4)
+    trial = np.tile(rec[:, :4], (10_000_000 // len(rec) + 1, 1))[:10_000_000]
+    for _ in range(3):
+        surrogate.exact_map(sc.prms, trial, fp64=False)
+        _, nfb, ms = surrogate.learned_map(sc.prms, params, norm, trial, tol=1e-2)
+    print(f"records {len(rec)} rows {len(trial)} learned ms {ms:.3f} fallbacks {nfb}")
+    return 0
+
+
 def main(argv):
     capi.load()
-    if len(argv) < 2 or argv[1] not in ("ensemble", "frame"):
+    if len(argv) < 2 or argv[1] not in ("ensemble", "frame", "learned"):
         print(__doc__)
         return 2
     if argv[1] == "ensemble":
         return ensemble(int(argv[2]) if len(argv) > 2 else 24)
+    if argv[1] == "learned":
+        return learned()
     return frame(len(argv) > 2 and argv[2] == "small")
 
 

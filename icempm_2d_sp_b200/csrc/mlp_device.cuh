@@ -5,9 +5,13 @@
 // MMAs (mma.sync m16n8k16, FP32 accumulate): rows 0-15 and 16-31 are two
 // m-tiles, the 64 hidden features eight n-tiles, and each layer's FP32
 // outputs become, after the activation, the BF16 A fragments of the next
-// layer in registers.  The weights sit in shared memory as BF16 pairs in the
-// B-fragment order (row n of W holds k, k+1 in one word), packed once per
-// network by k_mlp_pack.
+// layer in registers.  The weights sit in shared memory as B fragments: for
+// output row n and the k-tile of 16 inputs, lane (g, tg) = (lane / 4, lane % 4)
+// needs the BF16 pairs of inputs (2tg, 2tg+1) and (2tg+8, 2tg+9), which are
+// stored side by side as one 8-byte entry (one shared load per MMA operand).
+// The 16 entries of a row of W2 and W3 are swizzled, entry c at
+// c ^ 4 (n mod 4), so that the eight rows g a warp reads in one load fall on
+// different banks.  Packed once per network by k_mlp_pack.
 #pragma once
 #include <cstdint>
 #include <cuda_bf16.h>
@@ -22,9 +26,9 @@ constexpr int NPARAM = B3 + OUT;   // 4675
 
 // The packed network: what a CTA copies into shared memory.
 struct alignas(16) Packed {
-    uint32_t w1[HID][8];      // W1 as BF16 pairs, K padded 4 -> 16
-    uint32_t w2[HID][HID / 2];
-    uint32_t w3[8][HID / 2];  // N padded 3 -> 8
+    uint2 w1[HID][4];         // W1 fragments, K padded 4 -> 16 (one k-tile)
+    uint2 w2[HID][16];        // W2 fragments: 4 k-tiles x 4 lanes, swizzled
+    uint2 w3[8][16];          // W3 fragments, N padded 3 -> 8, swizzled
     float b1[HID], b2[HID], b3[8];
     float norm[16];           // x mean[4], x std[4], y mean[3], y std[3], 2 unused
 };
@@ -51,24 +55,31 @@ __device__ __forceinline__ void mma_bf16_16816(float (&d)[4], const uint32_t (&a
                  : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
 
+// Position of fragment entry c (k-tile c / 4, lane tg = c % 4) in row n.
+__host__ __device__ __forceinline__ int frag_slot(int n, int c) { return c ^ ((n & 3) << 2); }
+
 // One entry e of the packing of FP32 master parameters P and the
 // normalisation into a Packed network (entries 0 .. PACK_ENTRIES-1; every
 // word of the result is written by exactly one entry).
-constexpr int PACK_ENTRIES = HID * HID / 2;
+constexpr int PACK_ENTRIES = HID * 16;
 __device__ __forceinline__ void pack_entry(int e, const float *__restrict__ P, const float *__restrict__ norm,
                                            Packed &out)
 {
-    if (e < HID * 8) {                       // w1: k 2c, 2c+1 of row n (k >= IN is padding)
-        const int n = e / 8, c = e % 8, k = 2 * c;
-        out.w1[n][c] = pack_bf16x2(k < IN ? P[W1 + n * IN + k] : 0.0f, k + 1 < IN ? P[W1 + n * IN + k + 1] : 0.0f);
+    if (e < HID * 4) {                       // w1: inputs 2tg, 2tg+1 (and 2tg+8.. = padding) of row n
+        const int n = e / 4, k = 2 * (e % 4);
+        out.w1[n][e % 4] = make_uint2(pack_bf16x2(k < IN ? P[W1 + n * IN + k] : 0.0f,
+                                                  k + 1 < IN ? P[W1 + n * IN + k + 1] : 0.0f), 0u);
     }
-    {
-        const int n = e / (HID / 2), c = e % (HID / 2);
-        out.w2[n][c] = pack_bf16x2(P[W2 + n * HID + 2 * c], P[W2 + n * HID + 2 * c + 1]);
+    {                                        // w2: row n, k-tile kt, lane tg
+        const int n = e / 16, c = e % 16, k = 16 * (c / 4) + 2 * (c % 4);
+        const float *w = P + W2 + n * HID;
+        out.w2[n][frag_slot(n, c)] = make_uint2(pack_bf16x2(w[k], w[k + 1]), pack_bf16x2(w[k + 8], w[k + 9]));
     }
-    if (e < 8 * HID / 2) {                   // w3: rows n >= OUT are padding
-        const int n = e / (HID / 2), c = e % (HID / 2);
-        out.w3[n][c] = n < OUT ? pack_bf16x2(P[W3 + n * HID + 2 * c], P[W3 + n * HID + 2 * c + 1]) : 0u;
+    if (e < 8 * 16) {                        // w3: rows n >= OUT are padding
+        const int n = e / 16, c = e % 16, k = 16 * (c / 4) + 2 * (c % 4);
+        const float *w = P + W3 + n * HID;
+        out.w3[n][frag_slot(n, c)] = n < OUT ? make_uint2(pack_bf16x2(w[k], w[k + 1]), pack_bf16x2(w[k + 8], w[k + 9]))
+                                             : make_uint2(0u, 0u);
     }
     if (e < HID) { out.b1[e] = P[B1 + e]; out.b2[e] = P[B2 + e]; }
     if (e < 8) out.b3[e] = e < OUT ? P[B3 + e] : 0.0f;
@@ -118,8 +129,9 @@ __device__ __forceinline__ void rows_forward(const Packed &P, float (*io)[4], in
             const int n0 = (2 * kt) * 8, n1 = n0 + 8;
             c0[0] = P.b1[n0 + 2 * tg]; c0[1] = P.b1[n0 + 2 * tg + 1]; c0[2] = c0[0]; c0[3] = c0[1];
             c1[0] = P.b1[n1 + 2 * tg]; c1[1] = P.b1[n1 + 2 * tg + 1]; c1[2] = c1[0]; c1[3] = c1[1];
-            mma_bf16_16816(c0, ax, P.w1[n0 + g][tg], P.w1[n0 + g][tg + 4]);
-            mma_bf16_16816(c1, ax, P.w1[n1 + g][tg], P.w1[n1 + g][tg + 4]);
+            const uint2 b0 = P.w1[n0 + g][tg], b1 = P.w1[n1 + g][tg];
+            mma_bf16_16816(c0, ax, b0.x, b0.y);
+            mma_bf16_16816(c1, ax, b1.x, b1.y);
             a[kt][0] = silu_pack(c0[0], c0[1]);
             a[kt][1] = silu_pack(c0[2], c0[3]);
             a[kt][2] = silu_pack(c1[0], c1[1]);
@@ -136,15 +148,18 @@ __device__ __forceinline__ void rows_forward(const Packed &P, float (*io)[4], in
             c1[0] = P.b2[n1 + 2 * tg]; c1[1] = P.b2[n1 + 2 * tg + 1]; c1[2] = c1[0]; c1[3] = c1[1];
 #pragma unroll
             for (int k2 = 0; k2 < 4; k2++) {
-                mma_bf16_16816(c0, a[k2], P.w2[n0 + g][k2 * 8 + tg], P.w2[n0 + g][k2 * 8 + tg + 4]);
-                mma_bf16_16816(c1, a[k2], P.w2[n1 + g][k2 * 8 + tg], P.w2[n1 + g][k2 * 8 + tg + 4]);
+                const int slot = frag_slot(g, 4 * k2 + tg);   // rows n0 + g, n1 + g: n0, n1 multiples of 8
+                const uint2 b0 = P.w2[n0 + g][slot], b1 = P.w2[n1 + g][slot];
+                mma_bf16_16816(c0, a[k2], b0.x, b0.y);
+                mma_bf16_16816(c1, a[k2], b1.x, b1.y);
             }
             uint32_t a2[4];
             a2[0] = silu_pack(c0[0], c0[1]);
             a2[1] = silu_pack(c0[2], c0[3]);
             a2[2] = silu_pack(c1[0], c1[1]);
             a2[3] = silu_pack(c1[2], c1[3]);
-            mma_bf16_16816(d, a2, P.w3[g][kt * 8 + tg], P.w3[g][kt * 8 + tg + 4]);
+            const uint2 b3 = P.w3[g][frag_slot(g, 4 * kt + tg)];
+            mma_bf16_16816(d, a2, b3.x, b3.y);
         }
         // this m-tile's rows were read into the A fragments before its first MMA:
         // its outputs replace them (columns 2tg, 2tg+1 of rows g and g+8;

@@ -1167,14 +1167,18 @@ __device__ __noinline__ void learned_projection(const KParams<Real> &kp, mlp::Sm
 //     the return map, the stores of the new state, and the P2G source of the
 //     new state, written back into the point's own stage entries (A <- x, y,
 //     S1; H <- A, S0; K <- cell, mass).  The 3x3 node velocities (and the
-//     forcing entry) are loaded once per cell: after the locality sort a
-//     thread's points mostly share one cell.
+//     forcing entry) are loaded for every point; the locality sort gives a
+//     thread's points one cell, so all but the first load hit L1
+//     (ICEMPM_VEL_CACHE=1 keeps them in registers instead, which spills).
 //  2. per point: the source's node terms into the thread's register patch;
-//     then the patches go through the shared tile (the chunk's new cells +-1
-//     node) to the global accumulators.
-// Splitting the chunk keeps the velocity cache and the patch from being live
-// at the same time.  Every point of a chunk is read and written by the same
-// thread, so the stage entries need no barrier between the phases.
+//     at the end of the chunk the patches of vertically adjacent cells are
+//     merged with warp shuffles and every node channel goes to the global
+//     accumulators with one reduction (tile shapes: through the shared tile
+//     of the chunk's new cells +-1 node).
+// Splitting the chunk keeps the gather's and the return map's registers and
+// the patch from being live at the same time.  Every point of a chunk is read
+// and written by the same thread, so the stage entries need no barrier
+// between the phases.
 //
 // The gather is evaluated separably: with d_ab = v_ab - v_c (v_c the centre
 // node), S_a = sum_b wy_b d_ab and T_a = sum_b wy_b (b-1-y) d_ab,

@@ -119,8 +119,12 @@ public:
         sort_tmp_bytes_ = std::max(std::max(t32, t64), std::max(ts1, ts2));
         ICEMPM_CUDA(cudaMalloc(&sort_tmp_, sort_tmp_bytes_));
         // a CTA of the fused kernel handles BT*PPT points, ~BT*PPT/4 cells at
-        // 4 points per cell: 8 columns of BT*PPT/32 cells
-        tile_.tx = 8; tile_.ty = BT * PPT / 32;
+        // 4 points per cell: one column strip of BT*PPT/4 cells, so that a
+        // warp's 32 cells are 32 consecutive cells of one column (its
+        // reductions then form one contiguous run of nodes per node row and
+        // channel; fused kernel 0.500 ms with 8x16-cell tiles, 0.489 with 2x64,
+        // 0.485 with 1x128 on the 23M-point scene)
+        tile_.tx = 1; tile_.ty = BT * PPT / 4;
         tile_.ntiles_y = (gy_ + tile_.ty - 1) / tile_.ty;
         // persistent grid of the fused kernel: as many CTAs as fit on the device
         auto kern = k_g2p_p2g<Real, Acc, BT, PPT, CAP, STAGES, FUSED_PLAIN>;

@@ -1490,11 +1490,24 @@ __device__ __forceinline__ void fused_chunk(ChunkSmem<Real, Acc, BT, PPT, CAP, S
         bool low = true, high = true;
         patch_merge(patch, lane, low, high, false);
         if (patch.have) {
+            // the centre row; then one pass for the edge row each lane still
+            // owns (in a column run of cells only the run's ends own one: one
+            // pass of reductions for both ends instead of one per edge row),
+            // and a second one where a lane owns both (a cell without
+            // vertical neighbours)
 #pragma unroll
-            for (int a = 0; a < 3; a++)
+            for (int a = 0; a < 3; a++) patch_node<Real, Acc, CAP>(patch, T, G.acc, kp.gy, a, 1);
+            if (low || high) {
 #pragma unroll
-                for (int b = 0; b < 3; b++)
-                    if ((b != 0 || low) && (b != 2 || high)) patch_node<Real, Acc, CAP>(patch, T, G.acc, kp.gy, a, b);
+                for (int a = 0; a < 3; a++)
+                    node_add<Real, Acc, CAP>(T, patch.in_tile, G.acc, kp.gy, patch.cx + a - 1, patch.cy + (low ? -1 : 1),
+                                             low ? patch.m[a][0] : patch.m[a][2], low ? patch.p[a][0].x : patch.p[a][2].x,
+                                             low ? patch.p[a][0].y : patch.p[a][2].y);
+            }
+            if (low && high) {
+#pragma unroll
+                for (int a = 0; a < 3; a++) patch_node<Real, Acc, CAP>(patch, T, G.acc, kp.gy, a, 2);
+            }
         }
         // one stage: every thread has read its entries; refill the stage
         if (STAGES == 1) {

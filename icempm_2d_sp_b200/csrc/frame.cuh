@@ -165,8 +165,16 @@ __global__ void __launch_bounds__(256, 2) k_frame_scatter(Pts<Real> P, int n, in
             }
             if (mine) {
                 frame_node_add(F, gy, cx + a - 1, cy, add[1], add[1][kFrameChannels]);
-                if (!below) frame_node_add(F, gy, cx + a - 1, cy - 1, add[0], add[0][kFrameChannels]);
-                if (!above) frame_node_add(F, gy, cx + a - 1, cy + 1, add[2], add[2][kFrameChannels]);
+                // one pass for the edge node each lane still owns (in a column
+                // run of cells only the run's ends own one), a second where a
+                // lane owns both (a cell without vertical neighbours)
+                if (!below || !above) {
+                    float e[kFrameChannels + 1];
+#pragma unroll
+                    for (int c = 0; c <= kFrameChannels; c++) e[c] = !below ? add[0][c] : add[2][c];
+                    frame_node_add(F, gy, cx + a - 1, cy + (!below ? -1 : 1), e, e[kFrameChannels]);
+                }
+                if (!below && !above) frame_node_add(F, gy, cx + a - 1, cy + 1, add[2], add[2][kFrameChannels]);
             }
         }
     }

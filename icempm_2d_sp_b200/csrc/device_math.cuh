@@ -93,11 +93,11 @@ template <class T> struct Kin { T Jm1, J, d, b01; };
 template <class T> __device__ __forceinline__ Kin<T> kinematics(const M2<T> &H)
 {
     Kin<T> k;
-    k.Jm1 = (H.a00 + H.a11) + (H.a00 * H.a11 - H.a01 * H.a10);
+    k.Jm1 = fma(H.a00, H.a11, fma(-H.a01, H.a10, H.a00 + H.a11));
     k.J = T(1) + k.Jm1;
-    const T bm00 = T(2) * H.a00 + H.a00 * H.a00 + H.a01 * H.a01;
-    const T bm11 = T(2) * H.a11 + H.a10 * H.a10 + H.a11 * H.a11;
-    k.b01 = H.a01 + H.a10 + H.a00 * H.a10 + H.a01 * H.a11;
+    const T bm00 = fma(H.a00, H.a00, fma(H.a01, H.a01, T(2) * H.a00));
+    const T bm11 = fma(H.a10, H.a10, fma(H.a11, H.a11, T(2) * H.a11));
+    k.b01 = fma(H.a00, H.a10, fma(H.a01, H.a11, H.a01 + H.a10));
     k.d = T(0.5) * (bm00 - bm11);
     return k;
 }

